@@ -1,0 +1,164 @@
+#!/usr/bin/env python3
+"""Generate the committed golden fixtures from the read-only reference tree.
+
+Run once in a container that has the reference mounted, after
+`make -f oracle/Makefile.ref REF=<reference>`:
+
+    python tests/golden/make_golden.py --ref /root/reference
+
+Writes into tests/golden/:
+  scan-00000.vdw, quadruplets-00000.a4, scan-49900.vdw, quadruplets-49900.a4,
+  manifest.json      -- the reference's shipped sample blocks (data/sample/),
+                        copied byte for byte: encoder and decoder are checked
+                        against these exact bytes.
+  holdout32.json.gz  -- reproducibility/gpu_method/throughput/
+                        holdout-32-mr_selected.json windows[*].profiles_full,
+                        compacted to [p, [[r, M, L, K, w], ...]].
+  dense_oracle.json.gz -- the reference GPU dense-oracle records of
+                        reproducibility/gpu_method/night/ORACLES_NOUVEAUX.json
+                        and throughput/CONTROLES_INDEPENDANTS.json (p < 2^32).
+  refcpu_top_block.json.gz -- outputs of the reference's own CPU programs
+                        (oracle/_ref) on the 4096 primes ending at 4294967291:
+                        moment_worker A4 for all of them and the sparse CPU
+                        engine `advance adaptive p r 64 3 1` on a seeded
+                        sample of (p, r) pairs below block 49900.
+  refcpu_2p24.json.gz -- `independent p r 3` (full-walk reference) on a seeded
+                        sample of (p, r) pairs from the 4096 primes from 2^24,
+                        and moment_worker A4 for all 4096 of them.
+"""
+from __future__ import annotations
+
+import argparse
+import gzip
+import json
+import random
+import shutil
+import struct
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+sys.path.insert(0, str(REPO))
+import oracle  # noqa: E402  (checker, used here only to list primes)
+
+
+def dump(name, obj):
+    with gzip.open(HERE / name, "wt") as f:
+        json.dump(obj, f, separators=(",", ":"))
+
+
+def consecutive_primes_from(start, n):
+    out, x = [], start
+    while len(out) < n:
+        if oracle.is_prime(x):
+            out.append(x)
+        x += 1
+    return out
+
+
+def consecutive_primes_ending(top, n):
+    out, x = [], top
+    while len(out) < n:
+        if oracle.is_prime(x):
+            out.append(x)
+        x -= 1
+    return out[::-1]
+
+
+def moment_worker(ref_bin, primes):
+    vals = []
+    for i in range(0, len(primes), 4096):
+        chunk = primes[i:i + 4096]
+        line = f"0 -1 {len(chunk)} " + " ".join(map(str, chunk)) + "\nQUIT\n"
+        out = subprocess.run([str(ref_bin / "moment_worker")], input=line.encode(),
+                             capture_output=True, check=True).stdout
+        j = out.index(b"A4BATCH1")
+        hdr = out[j:j + 8 + 8 + 4 + 4 + 8 + 8 + 4 + 4 + 8 + 8]
+        n = struct.unpack_from("<I", hdr, 16)[0]
+        body = out[j + len(hdr): j + len(hdr) + 4 * n]
+        vals += list(struct.unpack("<" + "I" * n, body))
+    return vals
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--samples", type=int, default=48)
+    a = ap.parse_args()
+    ref = Path(a.ref)
+    ref_bin = REPO / "oracle" / "_ref"
+
+    for f in ["scan-00000.vdw", "quadruplets-00000.a4", "scan-49900.vdw",
+              "quadruplets-49900.a4", "manifest.json"]:
+        shutil.copyfile(ref / "data" / "sample" / f, HERE / f)
+
+    gm = ref / "reproducibility" / "gpu_method"
+    hold = json.loads((gm / "throughput" / "holdout-32-mr_selected.json").read_text())
+    windows = []
+    for w in hold["windows"]:
+        rows = [[row["p"], [[v["r"], v["max"], v["prefix"], v["K"], v["witness"]] for v in row["profiles"]]]
+                for row in w["profiles_full"]]
+        windows.append({"lo": w["lo"], "hi": w["hi"], "rows": rows})
+    dump("holdout32.json.gz", windows)
+
+    recs = {}
+    for rec in json.loads((gm / "night" / "ORACLES_NOUVEAUX.json").read_text()):
+        if rec["p"] < 2 ** 32 and rec.get("status") == "PASS":
+            recs[rec["p"]] = rec["profiles"]
+    for res in json.loads((gm / "throughput" / "CONTROLES_INDEPENDANTS.json").read_text())["results"]:
+        rec = res.get("oracle", {}).get("record", {})
+        if rec.get("p", 2 ** 40) < 2 ** 32 and rec.get("status") == "PASS":
+            recs[rec["p"]] = rec["profiles"]
+    dump("dense_oracle.json.gz", [[p, [[v["r"], v["max"], v["prefix"], v["K"], v["witness"]] for v in prof]]
+                                  for p, prof in sorted(recs.items())])
+
+    rng = random.Random(20261203)
+
+    # top block: 4096 primes ending at 4294967291
+    top = consecutive_primes_ending(4294967291, 4096)
+    a4_top = moment_worker(ref_bin, top)
+    below = [p for p in top if p < 4294915433]
+    pairs = []
+    while len(pairs) < a.samples:
+        p = rng.choice(below)
+        rs = [r for r in range(2, 10) if (p - 1) % r == 0]
+        pairs.append((p, rng.choice(rs)))
+
+    def run_adv(pr):
+        p, r = pr
+        out = subprocess.run([str(ref_bin / "advance"), "adaptive", str(p), str(r), "64", "3", "1"],
+                             capture_output=True, check=True, text=True).stdout
+        j = json.loads(out)
+        return [p, r, j["maximum"], j["prefix"], j["witness"]]
+
+    with ThreadPoolExecutor(8) as ex:
+        adv = list(ex.map(run_adv, pairs))
+    dump("refcpu_top_block.json.gz", {"primes": top, "a4": a4_top, "advance": adv})
+
+    # 2^24 block
+    low = consecutive_primes_from(2 ** 24, 4096)
+    a4_low = moment_worker(ref_bin, low)
+    pairs = []
+    while len(pairs) < a.samples:
+        p = rng.choice(low)
+        rs = [r for r in range(2, 10) if (p - 1) % r == 0]
+        pairs.append((p, rng.choice(rs)))
+
+    def run_ind(pr):
+        p, r = pr
+        out = subprocess.run([str(ref_bin / "independent"), str(p), str(r), "3"],
+                             capture_output=True, text=True).stdout
+        j = json.loads(out)
+        return [p, r, j["M"], j["L"], j["w"]]
+
+    with ThreadPoolExecutor(8) as ex:
+        ind = list(ex.map(run_ind, pairs))
+    dump("refcpu_2p24.json.gz", {"primes": low, "a4": a4_low, "independent": ind})
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

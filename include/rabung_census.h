@@ -1,0 +1,117 @@
+/*
+ * rabung_census.h -- C ABI of the B200 (sm_100a) power-residue census library
+ * (librabung_census.so).
+ *
+ * For every prime p and every r in {2..9} with r | p-1 the library computes
+ * the profile of the r-th power-residue colouring of 1..p-1: M (longest
+ * monochromatic run), L (initial run of the residue colour from x = 1), the
+ * canonical reflected witness min(s, p-(s+M-1)) over runs of length M, and
+ * the Rabung threshold K; optionally the quadratic A4 four-window count.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   - the census worker's per-prime computation behind its line protocol,
+ *     src/census/worker32.cu:10-45 (GPU) and src/census/small_cpu.cpp:15-40 (CPU);
+ *   - the A4 worker's per-prime count, src/census/moment_worker.cpp:19-52;
+ *   - the only in-process C ABI of the reference, baseline_init /
+ *     baseline_profile, src/census/engine32/src/baseline_bridge.cu:7,21-27.
+ *
+ * Conventions: caller-owned buffers; plain pointers and sizes; return 0 on
+ * success and a nonzero code on refusal, in which case outputs are invalid
+ * as a whole (no partial results, docs/METHODS.md:35 of the reference).
+ * One handle per host thread; a handle owns one CUDA stream.
+ */
+#ifndef RABUNG_CENSUS_H
+#define RABUNG_CENSUS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Mode flags for cz_census. */
+#define CZ_DENSE 1u   /* exhaustive half-interval scan (the dense oracle) */
+#define CZ_SPARSE 2u  /* certified rational-anchor filter */
+#define CZ_AUTO 3u    /* sparse for p >= sparse_min_p, dense below */
+#define CZ_A4 4u      /* also compute the quadratic A4 count */
+#define CZ_VERIFY 8u  /* certify every witness run and prefix by direct powers */
+
+/* Return codes. */
+#define CZ_OK 0
+#define CZ_EINVAL 1   /* bad argument (not prime, out of domain, buffer too small) */
+#define CZ_ECUDA 2    /* CUDA error */
+#define CZ_EREFUSED 3 /* a device status check failed: the whole request is refused */
+
+/* One (p, r) profile, 32 bytes.  Records come grouped by prime in input
+ * order and, within a prime, by ascending r. */
+typedef struct cz_profile {
+    uint32_t p, r;
+    uint32_t M;        /* longest monochromatic run */
+    uint32_t L;        /* initial residue run */
+    uint32_t witness;  /* least reflected start of a run of length M */
+    uint32_t status;   /* 0 */
+    uint64_t K;        /* Rabung threshold */
+} cz_profile;
+
+typedef struct cz_config {
+    int32_t device;          /* CUDA device ordinal */
+    uint32_t sparse_min_p;   /* CZ_AUTO routes p >= this to the anchor filter */
+    uint32_t cover_n;        /* cover shape: D ~ 2 sqrt(p/H) / cover_n (2..8) */
+    uint32_t q_cap[10];      /* cover window Q per order r (index r), 3..255 */
+    uint32_t anchor_bits;    /* anchor length: 32 r^-(t-1) <= 2^-anchor_bits */
+    uint32_t screen;         /* 1: bilateral screen after the anchor filter */
+    uint32_t sparse_blocks;  /* persistent filter grid (0: 2 per SM) */
+    uint32_t use_graph;      /* 1: replay device work through a captured CUDA graph */
+    uint32_t reserved[6];
+} cz_config;
+
+typedef struct cz_stats {
+    float ms_setup, ms_table, ms_sparse, ms_dense, ms_a4, ms_finalize, ms_device;
+    float ms_h2d, ms_d2h;
+    uint32_t n_primes, n_dense, n_sparse, n_profiles, n_fallback;
+    uint32_t kernels;               /* kernel launches of the call */
+    uint64_t words, completions;    /* sparse filter words visited, exact completions */
+    uint64_t h2d_bytes, d2h_bytes;
+} cz_stats;
+
+typedef struct cz_handle cz_handle;
+
+/* Fill *cfg with the defaults. */
+int cz_default_config(cz_config *cfg);
+
+/* Open a handle on cfg->device (allocates device tables); NULL cfg = defaults. */
+int cz_open(const cz_config *cfg, cz_handle **out);
+void cz_close(cz_handle *h);
+const char *cz_last_error(const cz_handle *h);
+
+/* Number of profiles (sum over primes of #{r in 2..9 : r | p-1}). */
+uint32_t cz_count_profiles(const uint32_t *primes, uint32_t n);
+
+/* Census of n primes (host buffers).  out must hold cz_count_profiles()
+ * records; a4_out (may be NULL unless CZ_A4) holds n values (0 for p = 2).
+ * stats may be NULL. */
+int cz_census(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags,
+              cz_profile *out, uint32_t out_cap, uint32_t *a4_out, cz_stats *stats);
+
+/* Re-run the device work of the previous cz_census call on its inputs, which
+ * are still resident in device memory (no host transfer, no planning); used
+ * to time the device path alone.  Results land in the same device buffers and
+ * are checked; stats receives the device times. */
+int cz_replay(cz_handle *h, cz_stats *stats);
+
+/* Quadratic A4 counts only (src/census/moment_worker.cpp:19-52 semantics):
+ * x in [1, p-4] with x..x+3 all of one quadratic character; 0 for p = 2. */
+int cz_a4(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t *a4_out);
+
+/* Reference-compatible adapter (src/census/engine32/src/baseline_bridge.cu:7,21-27):
+ * profile of one prime for the orders in `mask` (bit r-2), M into out[r] and
+ * L into prefix[r] (arrays of >= 10).  Returns 0, or 2 when mask asks for an
+ * order that does not divide p-1.  Not thread-safe (one global handle). */
+void baseline_init(unsigned cap);
+int baseline_profile(unsigned p, unsigned mask, unsigned *out, unsigned *prefix, int full);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RABUNG_CENSUS_H */

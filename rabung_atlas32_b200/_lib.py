@@ -1,0 +1,83 @@
+"""ctypes binding of librabung_census.so (include/rabung_census.h).
+
+The library is built in-tree (rabung_atlas32_b200/build.py).  Loading fails
+loudly when it is missing or no CUDA device is usable: there is no CPU
+fallback in the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+from .build import LIB
+
+CZ_DENSE, CZ_SPARSE, CZ_AUTO, CZ_A4, CZ_VERIFY = 1, 2, 3, 4, 8
+CZ_OK, CZ_EINVAL, CZ_ECUDA, CZ_EREFUSED = 0, 1, 2, 3
+
+u32, u64, i32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
+
+
+class cz_profile(ctypes.Structure):
+    _fields_ = [("p", u32), ("r", u32), ("M", u32), ("L", u32), ("witness", u32),
+                ("status", u32), ("K", u64)]
+
+
+class cz_config(ctypes.Structure):
+    _fields_ = [("device", i32), ("sparse_min_p", u32), ("cover_n", u32), ("q_cap", u32 * 10),
+                ("anchor_bits", u32), ("screen", u32), ("sparse_blocks", u32), ("use_graph", u32),
+                ("reserved", u32 * 6)]
+
+
+class cz_stats(ctypes.Structure):
+    _fields_ = [("ms_setup", ctypes.c_float), ("ms_table", ctypes.c_float), ("ms_sparse", ctypes.c_float),
+                ("ms_dense", ctypes.c_float), ("ms_a4", ctypes.c_float), ("ms_finalize", ctypes.c_float),
+                ("ms_device", ctypes.c_float), ("ms_h2d", ctypes.c_float), ("ms_d2h", ctypes.c_float),
+                ("n_primes", u32), ("n_dense", u32), ("n_sparse", u32), ("n_profiles", u32),
+                ("n_fallback", u32), ("kernels", u32), ("words", u64), ("completions", u64),
+                ("h2d_bytes", u64), ("d2h_bytes", u64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_count_profiles",
+           "cz_census", "cz_replay", "cz_a4", "baseline_init", "baseline_profile"]
+
+_lib = None
+
+
+def load(path: Path | str | None = None) -> ctypes.CDLL:
+    """Load the shared library (raises OSError if it is not built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB
+    if not p.exists():
+        raise OSError(f"{p} is not built; run `python -m rabung_atlas32_b200.build`")
+    L = ctypes.CDLL(str(p))
+    H = ctypes.c_void_p
+    L.cz_default_config.argtypes = [ctypes.POINTER(cz_config)]
+    L.cz_default_config.restype = ctypes.c_int
+    L.cz_open.argtypes = [ctypes.POINTER(cz_config), ctypes.POINTER(H)]
+    L.cz_open.restype = ctypes.c_int
+    L.cz_close.argtypes = [H]
+    L.cz_close.restype = None
+    L.cz_last_error.argtypes = [H]
+    L.cz_last_error.restype = ctypes.c_char_p
+    L.cz_count_profiles.argtypes = [ctypes.POINTER(u32), u32]
+    L.cz_count_profiles.restype = u32
+    L.cz_census.argtypes = [H, ctypes.POINTER(u32), u32, u32, ctypes.POINTER(cz_profile), u32,
+                            ctypes.POINTER(u32), ctypes.POINTER(cz_stats)]
+    L.cz_census.restype = ctypes.c_int
+    L.cz_replay.argtypes = [H, ctypes.POINTER(cz_stats)]
+    L.cz_replay.restype = ctypes.c_int
+    L.cz_a4.argtypes = [H, ctypes.POINTER(u32), u32, ctypes.POINTER(u32)]
+    L.cz_a4.restype = ctypes.c_int
+    L.baseline_init.argtypes = [ctypes.c_uint]
+    L.baseline_init.restype = None
+    L.baseline_profile.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),
+                                   ctypes.POINTER(ctypes.c_uint), ctypes.c_int]
+    L.baseline_profile.restype = ctypes.c_int
+    if path is None:
+        _lib = L
+    return L

@@ -1,0 +1,48 @@
+"""Build librabung_census.so in-tree with nvcc for sm_100a.
+
+    python -m rabung_atlas32_b200.build        (or build() from Python)
+
+The library is a plain C-ABI shared object (include/rabung_census.h); the
+Python package loads it with ctypes.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB = PKG / "librabung_census.so"
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+         "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
+
+
+def sources():
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "rabung_census.h"]
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    newest = max(p.stat().st_mtime for p in sources())
+    if LIB.exists() and not force and LIB.stat().st_mtime >= newest:
+        return LIB
+    tmp = LIB.with_suffix(f".{os.getpid()}.tmp.so")
+    cmd = [NVCC, *FLAGS, "-I", str(ROOT / "include"), "-o", str(tmp), str(CSRC / "census.cu")]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed for librabung_census.so")
+    if verbose:
+        sys.stderr.write(r.stderr)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,141 @@
+"""Python host API of the B200 census engine.
+
+`Census` wraps one library handle (one CUDA stream).  `profiles()` is the
+per-prime computation the reference census worker performs for each line of
+its protocol (src/census/worker32.cu:20-41): every admissible r, (M, L,
+witness, K), with the same refusal rule (a failed check refuses the whole
+request, docs/METHODS.md:35).  `block()` produces the reference's VDWSM1 /
+VDWA4V1 frames for an interval (docs/DATA_FORMAT.md).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+from . import _lib, codec
+
+MODES = {"dense": _lib.CZ_DENSE, "sparse": _lib.CZ_SPARSE, "auto": _lib.CZ_AUTO}
+
+
+class CensusError(RuntimeError):
+    """A refused request: no partial result is returned."""
+
+
+@dataclass
+class Tuning:
+    sparse_min_p: int = 1 << 20
+    cover_n: int = 3
+    q_cap: tuple = (0, 0, 40, 24, 20, 16, 16, 15, 14, 13)
+    anchor_bits: int = 4
+    screen: int = 1
+    sparse_blocks: int = 0
+    use_graph: int = 1
+
+
+def _as_u32_array(values):
+    arr = (ctypes.c_uint32 * len(values))()
+    for i, v in enumerate(values):
+        if not 0 <= int(v) < 2 ** 32:
+            raise ValueError(f"prime out of the 32-bit domain: {v}")
+        arr[i] = int(v)
+    return arr
+
+
+class Census:
+    def __init__(self, device: int = 0, tuning: Tuning | None = None):
+        self.lib = _lib.load()
+        cfg = _lib.cz_config()
+        self.lib.cz_default_config(ctypes.byref(cfg))
+        t = tuning or Tuning()
+        cfg.device = device
+        cfg.sparse_min_p = t.sparse_min_p
+        cfg.cover_n = t.cover_n
+        for r in range(10):
+            cfg.q_cap[r] = t.q_cap[r]
+        cfg.anchor_bits = t.anchor_bits
+        cfg.screen = t.screen
+        cfg.sparse_blocks = t.sparse_blocks
+        cfg.use_graph = t.use_graph
+        h = ctypes.c_void_p()
+        rc = self.lib.cz_open(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != 0:
+            raise CensusError(f"cz_open failed (rc={rc}): no usable CUDA device or bad tuning")
+        self.h = h
+        self.last_stats: dict = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cz_close(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _err(self) -> str:
+        return self.lib.cz_last_error(self.h).decode(errors="replace")
+
+    def count_profiles(self, primes) -> int:
+        arr = _as_u32_array(primes)
+        return int(self.lib.cz_count_profiles(arr, len(primes)))
+
+    def raw(self, primes, mode: str = "auto", a4: bool = True, verify: bool = False):
+        """Run the census; returns (ctypes profile array, A4 list or None, stats dict)."""
+        n = len(primes)
+        arr = _as_u32_array(primes)
+        nprof = int(self.lib.cz_count_profiles(arr, n))
+        out = (_lib.cz_profile * max(1, nprof))()
+        a4buf = (ctypes.c_uint32 * max(1, n))() if a4 else None
+        flags = MODES[mode] | (_lib.CZ_A4 if a4 else 0) | (_lib.CZ_VERIFY if verify else 0)
+        st = _lib.cz_stats()
+        rc = self.lib.cz_census(self.h, arr, n, flags, out, nprof, a4buf, ctypes.byref(st))
+        if rc != 0:
+            raise CensusError(f"census refused (rc={rc}): {self._err()}")
+        self.last_stats = st.as_dict()
+        return out, (list(a4buf[:n]) if a4 else None), self.last_stats
+
+    def profiles(self, primes, mode: str = "auto", a4: bool = True, verify: bool = False):
+        """List of codec.Record (profiles ascending r, A4 when requested)."""
+        out, a4v, _ = self.raw(primes, mode, a4, verify)
+        recs, k = [], 0
+        for i, p in enumerate(primes):
+            rec = codec.Record(int(p), [], a4v[i] if a4v else 0)
+            for _ in range(bin(codec.expected_mask(p)).count("1") if p > 2 else 0):
+                v = out[k]
+                k += 1
+                rec.profiles.append(codec.Profile(v.r, v.M, v.L, v.witness, v.K))
+            recs.append(rec)
+        return recs
+
+    def replay(self) -> dict:
+        """Re-run the device work of the last call on its resident inputs."""
+        st = _lib.cz_stats()
+        rc = self.lib.cz_replay(self.h, ctypes.byref(st))
+        if rc != 0:
+            raise CensusError(f"replay refused (rc={rc}): {self._err()}")
+        return st.as_dict()
+
+    def a4(self, primes) -> list:
+        n = len(primes)
+        arr = _as_u32_array(primes)
+        buf = (ctypes.c_uint32 * max(1, n))()
+        rc = self.lib.cz_a4(self.h, arr, n, buf)
+        if rc != 0:
+            raise CensusError(f"A4 refused (rc={rc}): {self._err()}")
+        return list(buf[:n])
+
+    def block(self, lo: int, hi: int, primes=None, mode: str = "auto"):
+        """(scan_frame, a4_frame, records) for the primes of [lo, hi)."""
+        if primes is None:
+            from .sieve import primes_in
+            primes = primes_in(lo, hi)
+        recs = self.profiles(primes, mode=mode, a4=True)
+        return codec.encode_scan_frame(lo, hi, recs), codec.encode_a4_frame(lo, hi, recs), recs

@@ -1,0 +1,675 @@
+// census.cu -- host orchestration and C ABI of librabung_census.so.
+//
+// One call (cz_census) takes a batch of primes through:
+//   plan (host, O(n)): admissible orders, route (dense / sparse), cover
+//     (B, D_r, Q_r) by the integer certificate, plane and summary layout;
+//   setup_kernel: primality, Montgomery constants, roots of unity;
+//   table_kernel + sparse_kernel: signed planes, persistent anchor filter;
+//   dense_scan_kernel + dense_merge_kernel: exhaustive half-interval scan;
+//   finalize_kernel: prefix, optional direct certification, K, records;
+//   a4_kernel: quadratic A4 counts.
+// The device work of the last call can be replayed on resident inputs
+// (cz_replay), optionally through a captured CUDA graph.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "labels.cuh"
+#include "dense.cuh"
+#include "table.cuh"
+#include "sparse.cuh"
+#include "finalize.cuh"
+#include "a4.cuh"
+#include "../../include/rabung_census.h"
+
+using namespace cz;
+
+namespace {
+
+constexpr u32 CHAIN_LIMIT = (1u << 20) + 8192u;   // table labels cover n < CHAIN_LIMIT
+constexpr u32 B_MAX = (1u << 20);
+
+struct Buf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+bool cover_cert(u64 B, u64 D, u64 H, u64 p) {
+    if (H * D > 2 * B) return false;
+    const unsigned __int128 lhs = (unsigned __int128)4 * B * D - (unsigned __int128)H * D * D;
+    return lhs > (unsigned __int128)4 * p;
+}
+
+// table radius for a prime: D = floor(2 sqrt(p/H) / n), B = floor((4p + H D^2)/(4D)) + 1
+// (the reference's lower-branch choice, paper/GPU_METHOD_EN.tex "Choosing parameters";
+// P/src/clipped_cover.hpp:14-21), certified in integers.
+bool cover_B(u32 p, u32 Q, u32 ndiv, u32 &Bout) {
+    const u64 H = Q - 1u;
+    const double D0 = 2.0 * std::sqrt((double)p / (double)H);
+    u64 D = (u64)(D0 / (double)ndiv);
+    if (D < 1) D = 1;
+    const u64 B = (4ull * p + H * D * D) / (4ull * D) + 1ull;
+    if (B >= p || D >= p || B > B_MAX) return false;
+    if (!cover_cert(B, D, H, p)) return false;
+    Bout = (u32)B;
+    return true;
+}
+
+// least D with the certificate for (p, B, Q)
+bool cover_D(u32 p, u32 B, u32 Q, u32 &Dout) {
+    const u64 H = Q - 1u;
+    const long double disc = (long double)B * B - (long double)H * p;
+    if (disc <= 0) return false;
+    long double est = (2.0L * B - 2.0L * std::sqrt(disc)) / (long double)H;
+    u64 D = est < 1 ? 1 : (u64)est;
+    while (D > 1 && cover_cert(B, D - 1, H, p)) --D;
+    while (!cover_cert(B, D, H, p)) {
+        ++D;
+        if (H * D > 2ull * B || D >= p || D > B_MAX) return false;
+    }
+    Dout = (u32)D;
+    return true;
+}
+
+u32 popc(u32 x) { return (u32)__builtin_popcount(x); }
+
+}  // namespace
+
+struct cz_handle {
+    cz_config cfg{};
+    int dev = 0;
+    int sms = 148;
+    cudaStream_t st = nullptr;
+    std::string err;
+    u32 *d_small = nullptr;
+    uint2 *d_chain = nullptr;
+    u32 n_small = 0;
+    // device buffers
+    Buf b_in, b_primes, b_profs, b_state, b_planes, b_summ, b_chunk, b_summp, b_didx, b_sidx,
+        b_slist, b_dlist, b_dpre, b_out, b_a4, b_counter;
+    // host copies of the current plan
+    std::vector<PrimeDesc> hp;
+    std::vector<ProfDesc> hprof;
+    std::vector<u32> h_chunk, h_summp, h_didx, h_sidx, h_slist, h_dlist;
+    u32 n = 0, nprof = 0, ndense = 0, nsparse = 0, nchunks = 0, nsl = 0, ndl = 0;
+    u32 table_smem = 0, dense_smem = 0;
+    u32 flags = 0;
+    bool have_plan = false;
+    cudaEvent_t ev[10]{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cz_stats last{};
+    std::vector<OutRecord> hout;
+};
+
+namespace {
+
+bool ck(cz_handle *h, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return true;
+    h->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+}
+
+bool ensure(cz_handle *h, Buf &b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return true;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t want = bytes + bytes / 4;
+    if (!ck(h, cudaMalloc(&b.p, want), "cudaMalloc")) return false;
+    b.cap = want;
+    return true;
+}
+
+template <class T> T *P(Buf &b) { return reinterpret_cast<T *>(b.p); }
+
+bool build_static_tables(cz_handle *h) {
+    // primes below CHAIN_LIMIT and the smallest-prime-factor chain
+    std::vector<u32> spf(CHAIN_LIMIT, 0);
+    std::vector<u32> primes;
+    for (u32 i = 2; i < CHAIN_LIMIT; ++i) {
+        if (!spf[i]) {
+            spf[i] = i;
+            primes.push_back(i);
+            if ((u64)i * i < CHAIN_LIMIT)
+                for (u32 j = i * i; j < CHAIN_LIMIT; j += i)
+                    if (!spf[j]) spf[j] = i;
+        }
+    }
+    std::vector<u32> index(CHAIN_LIMIT, 0);
+    for (u32 k = 0; k < primes.size(); ++k) index[primes[k]] = k;
+    std::vector<uint2> chain(CHAIN_LIMIT);
+    chain[0] = make_uint2(0, 0);
+    chain[1] = make_uint2(0, 1);
+    for (u32 n = 2; n < CHAIN_LIMIT; ++n) chain[n] = make_uint2(index[spf[n]], n / spf[n]);
+    h->n_small = (u32)primes.size();
+    if (!ck(h, cudaMalloc(&h->d_small, primes.size() * 4), "cudaMalloc small")) return false;
+    if (!ck(h, cudaMalloc(&h->d_chain, chain.size() * sizeof(uint2)), "cudaMalloc chain")) return false;
+    if (!ck(h, cudaMemcpy(h->d_small, primes.data(), primes.size() * 4, cudaMemcpyHostToDevice), "copy small")) return false;
+    if (!ck(h, cudaMemcpy(h->d_chain, chain.data(), chain.size() * sizeof(uint2), cudaMemcpyHostToDevice), "copy chain")) return false;
+    return true;
+}
+
+u32 q_for(const cz_config &c, u32 r) { return c.q_cap[r] ? c.q_cap[r] : 16u; }
+
+// host plan of one call
+int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
+    const cz_config &c = h->cfg;
+    h->hp.assign(n, PrimeDesc{});
+    h->hprof.clear();
+    h->h_didx.clear(); h->h_sidx.clear(); h->h_slist.clear(); h->h_dlist.clear();
+    h->h_chunk.assign(1, 0u); h->h_summp.clear();
+    u64 plane_words = 0;
+    u32 max_slots_t = 8, max_slots_d = 8, max_nq = 0;
+    u64 summ_slots = 0;
+    const u32 mode = flags & CZ_AUTO;
+    for (u32 i = 0; i < n; ++i) {
+        const u32 p = primes[i];
+        if (p < 2u) { h->err = "prime out of domain: " + std::to_string(p); return CZ_EINVAL; }
+        PrimeDesc &P = h->hp[i];
+        P.p = p;
+        P.mask = p > 2u ? mask_of(p) : 0u;
+        P.m = lcm_of_mask(P.mask);
+        P.e = P.mask ? (p - 1u) / P.m : 0u;
+        P.first_prof = (u32)h->hprof.size();
+        P.nprof = popc(P.mask);
+        P.route = 0;
+        if (!P.nprof) continue;
+        bool sparse = false;
+        if (mode == CZ_SPARSE) sparse = true;
+        else if (mode == CZ_AUTO) sparse = p >= c.sparse_min_p;
+        u32 B = 0, Qmax = 0;
+        std::vector<u32> Ds;
+        if (sparse) {
+            for (u32 r = 2; r <= 9; ++r)
+                if (P.mask & (1u << (r - 2))) Qmax = std::max(Qmax, q_for(c, r));
+            if (p < 4096u || Qmax + 1u >= p || !cover_B(p, Qmax, c.cover_n, B)) sparse = false;
+            if (sparse) {
+                for (u32 r = 2; r <= 9 && sparse; ++r) {
+                    if (!(P.mask & (1u << (r - 2)))) continue;
+                    u32 D = 0;
+                    if (!cover_D(p, B, q_for(c, r), D)) sparse = false;
+                    Ds.push_back(D);
+                }
+            }
+            if (!sparse && mode == CZ_SPARSE) {
+                h->err = "sparse path unsupported for p = " + std::to_string(p);
+                return CZ_EINVAL;
+            }
+        }
+        P.route = sparse ? 2u : 1u;
+        if (sparse) {
+            P.B = B;
+            P.K0 = (B + 31u) / 32u + 4u;
+            P.nwords = 2u * P.K0 + 8u;
+            h->h_sidx.push_back(i);
+            max_slots_t = std::max(max_slots_t, hash_slots(P.m));
+        } else {
+            const u32 nh = (p - 1u) / 2u;
+            const u32 nseg = (nh + DENSE_SEG - 1u) / DENSE_SEG;
+            const u32 nch = (nseg + DENSE_WARPS - 1u) / DENSE_WARPS;
+            h->h_didx.push_back(i);
+            h->h_summp.push_back((u32)summ_slots);
+            summ_slots += (u64)nch * P.nprof;
+            h->h_chunk.push_back(h->h_chunk.back() + nch);
+            max_slots_d = std::max(max_slots_d, hash_slots(P.m));
+        }
+        u32 k = 0;
+        for (u32 r = 2; r <= 9; ++r) {
+            if (!(P.mask & (1u << (r - 2)))) continue;
+            ProfDesc D{};
+            D.prime = i;
+            D.r = r;
+            D.np = planes_for(r);
+            D.out_slot = (u32)h->hprof.size();
+            if (sparse) {
+                D.Q = q_for(c, r);
+                D.D = Ds[k];
+                D.plane_off = plane_words;
+                plane_words += (u64)D.np * P.nwords;
+                D.local = (u32)h->h_sidx.size() - 1u;
+                h->h_slist.push_back((u32)h->hprof.size());
+            } else {
+                D.local = (u32)h->h_didx.size() - 1u;
+                h->h_dlist.push_back((u32)h->hprof.size());
+            }
+            h->hprof.push_back(D);
+            ++k;
+        }
+    }
+    h->n = n;
+    h->nprof = (u32)h->hprof.size();
+    h->ndense = (u32)h->h_didx.size();
+    h->nsparse = (u32)h->h_sidx.size();
+    h->nchunks = h->h_chunk.back();
+    h->nsl = (u32)h->h_slist.size();
+    h->ndl = (u32)h->h_dlist.size();
+    // primes below the largest table end, for the table kernel's shared memory
+    u32 maxB = 0;
+    for (u32 i : h->h_sidx) maxB = std::max(maxB, h->hp[i].B);
+    if (h->nsparse) {
+        const u32 nmax = 32u * ((maxB + 1u + 31u) / 32u + 1u);
+        // count primes below nmax on the host (static table is sorted)
+        static std::vector<u32> hs;
+        static std::once_flag once;
+        std::call_once(once, [] {
+            std::vector<char> comp(CHAIN_LIMIT, 0);
+            for (u32 i = 2; i < CHAIN_LIMIT; ++i)
+                if (!comp[i]) {
+                    hs.push_back(i);
+                    if ((u64)i * i < CHAIN_LIMIT)
+                        for (u32 j = i * i; j < CHAIN_LIMIT; j += i) comp[j] = 1;
+                }
+        });
+        max_nq = (u32)(std::lower_bound(hs.begin(), hs.end(), nmax) - hs.begin());
+    }
+    h->table_smem = max_slots_t * 6u + 8u + max_nq * 2u + 16u;
+    h->dense_smem = max_slots_d * 6u + 16u;
+    // device buffers
+    if (!ensure(h, h->b_primes, sizeof(PrimeDesc) * n) ||
+        !ensure(h, h->b_profs, sizeof(ProfDesc) * h->nprof) ||
+        !ensure(h, h->b_state, sizeof(ProfState) * h->nprof) ||
+        !ensure(h, h->b_planes, plane_words * 4ull) ||
+        !ensure(h, h->b_summ, sizeof(Summ) * summ_slots) ||
+        !ensure(h, h->b_chunk, 4ull * h->h_chunk.size()) ||
+        !ensure(h, h->b_summp, 4ull * h->h_summp.size()) ||
+        !ensure(h, h->b_didx, 4ull * h->ndense) ||
+        !ensure(h, h->b_sidx, 4ull * h->nsparse) ||
+        !ensure(h, h->b_slist, 4ull * h->nsl) ||
+        !ensure(h, h->b_dlist, 4ull * h->ndl) ||
+        !ensure(h, h->b_dpre, 4ull * h->nprof) ||
+        !ensure(h, h->b_out, sizeof(OutRecord) * h->nprof) ||
+        !ensure(h, h->b_a4, 4ull * n) ||
+        !ensure(h, h->b_counter, 64))
+        return CZ_ECUDA;
+    h->flags = flags;
+    h->have_plan = true;
+    return CZ_OK;
+}
+
+int upload(cz_handle *h, cz_stats *s) {
+    cudaStream_t st = h->st;
+    size_t bytes = 0;
+    auto put = [&](Buf &b, const void *src, size_t n) {
+        bytes += n;
+        return n == 0 || ck(h, cudaMemcpyAsync(b.p, src, n, cudaMemcpyHostToDevice, st), "h2d");
+    };
+    if (!put(h->b_primes, h->hp.data(), sizeof(PrimeDesc) * h->n) ||
+        !put(h->b_profs, h->hprof.data(), sizeof(ProfDesc) * h->nprof) ||
+        !put(h->b_chunk, h->h_chunk.data(), 4ull * h->h_chunk.size()) ||
+        !put(h->b_summp, h->h_summp.data(), 4ull * h->h_summp.size()) ||
+        !put(h->b_didx, h->h_didx.data(), 4ull * h->ndense) ||
+        !put(h->b_sidx, h->h_sidx.data(), 4ull * h->nsparse) ||
+        !put(h->b_slist, h->h_slist.data(), 4ull * h->nsl) ||
+        !put(h->b_dlist, h->h_dlist.data(), 4ull * h->ndl))
+        return CZ_ECUDA;
+    if (s) s->h2d_bytes = bytes;
+    return CZ_OK;
+}
+
+// enqueue the device work of the current plan on h->st; returns launches
+int enqueue(cz_handle *h, bool timed, u32 &launches) {
+    cudaStream_t st = h->st;
+    launches = 0;
+    auto rec = [&](int i) { if (timed) cudaEventRecord(h->ev[i], st); };
+    rec(0);
+    if (h->n) {
+        setup_kernel<<<(h->n + 127) / 128, 128, 0, st>>>(P<PrimeDesc>(h->b_primes), P<ProfDesc>(h->b_profs),
+                                                         P<ProfState>(h->b_state), h->n);
+        ++launches;
+    }
+    rec(1);
+    if (h->nsparse) {
+        TableArgs ta;
+        ta.primes = P<PrimeDesc>(h->b_primes);
+        ta.profs = P<ProfDesc>(h->b_profs);
+        ta.state = P<ProfState>(h->b_state);
+        ta.planes = P<u32>(h->b_planes);
+        ta.sparse_primes = P<u32>(h->b_sidx);
+        ta.nsparse = h->nsparse;
+        ta.small_primes = h->d_small;
+        ta.n_small = h->n_small;
+        ta.chain = h->d_chain;
+        ta.chain_limit = CHAIN_LIMIT;
+        const u32 grid = std::min<u32>(h->nsparse, (u32)h->sms);
+        table_kernel<<<grid, TABLE_THREADS, h->table_smem, st>>>(ta);
+        ++launches;
+    }
+    rec(2);
+    if (h->nsl) {
+        cudaMemsetAsync(h->b_counter.p, 0, 64, st);
+        SparseArgs sa;
+        sa.primes = P<PrimeDesc>(h->b_primes);
+        sa.profs = P<ProfDesc>(h->b_profs);
+        sa.state = P<ProfState>(h->b_state);
+        sa.planes = P<u32>(h->b_planes);
+        sa.prof_list = P<u32>(h->b_slist);
+        sa.nlist = h->nsl;
+        sa.next = P<u32>(h->b_counter);
+        sa.tune.anchor_bits = h->cfg.anchor_bits;
+        sa.tune.screen = h->cfg.screen;
+        u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : 2u * (u32)h->sms;
+        grid = std::min(grid, h->nsl);
+        sparse_kernel<<<grid, SPARSE_WARPS * 32, 0, st>>>(sa);
+        ++launches;
+    }
+    rec(3);
+    if (h->ndense) {
+        DenseArgs da;
+        da.primes = P<PrimeDesc>(h->b_primes);
+        da.dense_idx = P<u32>(h->b_didx);
+        da.profs = P<ProfDesc>(h->b_profs);
+        da.chunk_prefix = P<u32>(h->b_chunk);
+        da.summ_prefix = P<u32>(h->b_summp);
+        da.nprimes = h->ndense;
+        da.nchunks = h->nchunks;
+        da.summ = P<Summ>(h->b_summ);
+        da.state = P<ProfState>(h->b_state);
+        const u32 grid = std::min<u32>(h->nchunks, (u32)h->sms * 8u);
+        dense_scan_kernel<<<grid, DENSE_WARPS * 32, h->dense_smem, st>>>(da);
+        DenseMergeArgs ma;
+        ma.primes = P<PrimeDesc>(h->b_primes);
+        ma.profs = P<ProfDesc>(h->b_profs);
+        ma.chunk_prefix = P<u32>(h->b_chunk);
+        ma.summ_prefix = P<u32>(h->b_summp);
+        ma.nprimes = h->ndense;
+        ma.summ = P<Summ>(h->b_summ);
+        ma.state = P<ProfState>(h->b_state);
+        ma.prefix_out = P<u32>(h->b_dpre);
+        dense_merge_kernel<<<(h->ndl + 7) / 8, 256, 0, st>>>(ma, P<u32>(h->b_dlist), h->ndl);
+        launches += 2;
+    }
+    rec(4);
+    if (h->nprof) {
+        finalize_kernel<<<(h->nprof + 127) / 128, 128, 0, st>>>(
+            P<PrimeDesc>(h->b_primes), P<ProfDesc>(h->b_profs), P<ProfState>(h->b_state), P<u32>(h->b_dpre),
+            h->nprof, (h->flags & CZ_VERIFY) ? 1u : 0u, P<OutRecord>(h->b_out));
+        ++launches;
+    }
+    rec(5);
+    if ((h->flags & CZ_A4) && h->n) {
+        a4_kernel<<<(h->n + A4_WARPS - 1) / A4_WARPS, A4_WARPS * 32, 0, st>>>(P<PrimeDesc>(h->b_primes), h->n,
+                                                                           P<u32>(h->b_a4), P<u32>(h->b_counter) + 8);
+        ++launches;
+    }
+    rec(6);
+    return ck(h, cudaGetLastError(), "launch") ? CZ_OK : CZ_ECUDA;
+}
+
+void read_times(cz_handle *h, cz_stats *s) {
+    float t[6] = {0};
+    for (int i = 0; i < 6; ++i) cudaEventElapsedTime(&t[i], h->ev[i], h->ev[i + 1]);
+    s->ms_setup = t[0]; s->ms_table = t[1]; s->ms_sparse = t[2]; s->ms_dense = t[3];
+    s->ms_finalize = t[4]; s->ms_a4 = t[5];
+    cudaEventElapsedTime(&s->ms_device, h->ev[0], h->ev[6]);
+}
+
+int check_records(cz_handle *h, std::vector<u32> *fallback) {
+    for (u32 g = 0; g < h->nprof; ++g) {
+        const OutRecord &o = h->hout[g];
+        if (o.status) {
+            const PrimeDesc &P = h->hp[h->hprof[g].prime];
+            if (fallback && P.route == 2u && !(o.status & (ST_ROOT | ST_LABEL | ST_VERIFY))) {
+                if (fallback->empty() || fallback->back() != h->hprof[g].prime)
+                    fallback->push_back(h->hprof[g].prime);
+                continue;
+            }
+            char buf[160];
+            snprintf(buf, sizeof buf, "refused: p=%u r=%u status=0x%x", o.p, o.r, o.status);
+            h->err = buf;
+            return CZ_EREFUSED;
+        }
+    }
+    return CZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cz_default_config(cz_config *c) {
+    if (!c) return CZ_EINVAL;
+    std::memset(c, 0, sizeof *c);
+    c->device = 0;
+    c->sparse_min_p = 1u << 20;
+    c->cover_n = 3;
+    const u32 q[10] = {0, 0, 40, 24, 20, 16, 16, 15, 14, 13};
+    for (int r = 0; r < 10; ++r) c->q_cap[r] = q[r];
+    c->anchor_bits = 4;
+    c->screen = 1;
+    c->sparse_blocks = 0;
+    c->use_graph = 1;
+    return CZ_OK;
+}
+
+int cz_open(const cz_config *cfg, cz_handle **out) {
+    if (!out) return CZ_EINVAL;
+    *out = nullptr;
+    cz_handle *h = new cz_handle();
+    if (cfg) h->cfg = *cfg; else cz_default_config(&h->cfg);
+    if (h->cfg.cover_n < 2 || h->cfg.cover_n > 8) { delete h; return CZ_EINVAL; }
+    for (int r = 2; r <= 9; ++r)
+        if (h->cfg.q_cap[r] && (h->cfg.q_cap[r] < 3 || h->cfg.q_cap[r] > 255)) { delete h; return CZ_EINVAL; }
+    h->dev = h->cfg.device;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || h->dev < 0 || h->dev >= ndev) { delete h; return CZ_ECUDA; }
+    cudaSetDevice(h->dev);
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, h->dev);
+    h->sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) { delete h; return CZ_ECUDA; }
+    for (auto &e : h->ev) cudaEventCreate(&e);
+    cudaFuncSetAttribute(table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(dense_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    if (!build_static_tables(h)) { cz_close(h); return CZ_ECUDA; }
+    *out = h;
+    return CZ_OK;
+}
+
+void cz_close(cz_handle *h) {
+    if (!h) return;
+    cudaSetDevice(h->dev);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    Buf *bufs[] = {&h->b_in, &h->b_primes, &h->b_profs, &h->b_state, &h->b_planes, &h->b_summ, &h->b_chunk,
+                   &h->b_summp, &h->b_didx, &h->b_sidx, &h->b_slist, &h->b_dlist, &h->b_dpre, &h->b_out,
+                   &h->b_a4, &h->b_counter};
+    for (Buf *b : bufs) if (b->p) cudaFree(b->p);
+    if (h->d_small) cudaFree(h->d_small);
+    if (h->d_chain) cudaFree(h->d_chain);
+    for (auto &e : h->ev) if (e) cudaEventDestroy(e);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+const char *cz_last_error(const cz_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+uint32_t cz_count_profiles(const uint32_t *primes, uint32_t n) {
+    u32 c = 0;
+    for (u32 i = 0; i < n; ++i)
+        if (primes[i] > 2u) c += popc(mask_of(primes[i]));
+    return c;
+}
+
+static int census_impl(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags, cz_profile *out,
+                       uint32_t out_cap, uint32_t *a4_out, cz_stats *stats, bool allow_fallback) {
+    if (!h) return CZ_EINVAL;
+    cudaSetDevice(h->dev);
+    h->err.clear();
+    cz_stats s{};
+    if (n == 0) { if (stats) *stats = s; return CZ_OK; }
+    if (!primes || !out || ((flags & CZ_A4) && !a4_out)) { h->err = "null buffer"; return CZ_EINVAL; }
+    if ((flags & CZ_AUTO) == 0) flags |= CZ_AUTO;
+    const u32 need = cz_count_profiles(primes, n);
+    if (out_cap < need) { h->err = "output capacity below profile count"; return CZ_EINVAL; }
+    int rc = plan(h, primes, n, flags);
+    if (rc) return rc;
+    if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0); cudaEventCreate(&t1);
+    cudaEventRecord(t0, h->st);
+    if ((rc = upload(h, &s))) return rc;
+    cudaEventRecord(t1, h->st);
+    u32 launches = 0;
+    if ((rc = enqueue(h, true, launches))) return rc;
+    h->hout.resize(h->nprof);
+    cudaEvent_t t2;
+    cudaEventCreate(&t2);
+    if (h->nprof && !ck(h, cudaMemcpyAsync(h->hout.data(), h->b_out.p, sizeof(OutRecord) * h->nprof,
+                                           cudaMemcpyDeviceToHost, h->st), "d2h"))
+        return CZ_ECUDA;
+    if ((flags & CZ_A4) && !ck(h, cudaMemcpyAsync(a4_out, h->b_a4.p, 4ull * n, cudaMemcpyDeviceToHost, h->st), "d2h a4"))
+        return CZ_ECUDA;
+    cudaEventRecord(t2, h->st);
+    if (!ck(h, cudaStreamSynchronize(h->st), "census")) return CZ_ECUDA;
+    cudaEventElapsedTime(&s.ms_h2d, t0, t1);
+    cudaEventElapsedTime(&s.ms_d2h, h->ev[6], t2);
+    cudaEventDestroy(t0); cudaEventDestroy(t1); cudaEventDestroy(t2);
+    read_times(h, &s);
+    s.d2h_bytes = sizeof(OutRecord) * h->nprof + ((flags & CZ_A4) ? 4ull * n : 0ull);
+    s.n_primes = n; s.n_dense = h->ndense; s.n_sparse = h->nsparse; s.n_profiles = h->nprof;
+    s.kernels = launches;
+    {
+        std::vector<ProfState> hs(h->nprof);
+        if (h->nprof) cudaMemcpy(hs.data(), h->b_state.p, sizeof(ProfState) * h->nprof, cudaMemcpyDeviceToHost);
+        for (auto &x : hs) { s.words += x.words; s.completions += x.completions; }
+    }
+    if (flags & CZ_A4) {
+        u32 a4err = 0;
+        cudaMemcpy(&a4err, P<u32>(h->b_counter) + 8, 4, cudaMemcpyDeviceToHost);
+        if (a4err) { h->err = "refused: A4 point count not certified"; return CZ_EREFUSED; }
+    }
+    std::vector<u32> fb;
+    rc = check_records(h, allow_fallback ? &fb : nullptr);
+    if (rc) return rc;
+    for (u32 g = 0; g < h->nprof; ++g) {
+        const OutRecord &o = h->hout[g];
+        cz_profile &d = out[g];
+        d.p = o.p; d.r = o.r; d.M = o.M; d.L = o.L; d.witness = o.witness; d.status = o.status; d.K = o.K;
+    }
+    if (!fb.empty()) {
+        // sparse primes whose seed could not certify a threshold: dense re-run
+        std::vector<u32> sub, slot;
+        for (u32 pi : fb) sub.push_back(h->hp[pi].p);
+        std::vector<u32> first(fb.size());
+        for (size_t k = 0; k < fb.size(); ++k) first[k] = h->hp[fb[k]].first_prof;
+        const u32 fflags = (flags & ~CZ_AUTO & ~CZ_A4) | CZ_DENSE;
+        std::vector<cz_profile> tmp(cz_count_profiles(sub.data(), (u32)sub.size()));
+        cz_stats s2{};
+        std::vector<OutRecord> keep_out = h->hout;
+        rc = census_impl(h, sub.data(), (u32)sub.size(), fflags, tmp.data(), (u32)tmp.size(), nullptr, &s2, false);
+        if (rc) return rc;
+        u32 t = 0;
+        for (size_t k = 0; k < fb.size(); ++k) {
+            const u32 np = popc(mask_of(sub[k]));
+            for (u32 j = 0; j < np; ++j) out[first[k] + j] = tmp[t++];
+        }
+        s.n_fallback = (u32)fb.size();
+        h->have_plan = false;   // the plan now describes the fallback batch
+    }
+    h->last = s;
+    if (stats) *stats = s;
+    return CZ_OK;
+}
+
+int cz_census(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags, cz_profile *out,
+              uint32_t out_cap, uint32_t *a4_out, cz_stats *stats) {
+    return census_impl(h, primes, n, flags, out, out_cap, a4_out, stats, true);
+}
+
+int cz_replay(cz_handle *h, cz_stats *stats) {
+    if (!h || !h->have_plan) { if (h) h->err = "no resident plan to replay"; return CZ_EINVAL; }
+    cudaSetDevice(h->dev);
+    cz_stats s{};
+    u32 launches = 0;
+    int rc;
+    if (h->cfg.use_graph) {
+        if (!h->gexec) {
+            if (!ck(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal), "capture")) return CZ_ECUDA;
+            rc = enqueue(h, false, launches);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(h->st, &g);
+            if (rc || !ck(h, e, "end capture")) return CZ_ECUDA;
+            h->graph = g;
+            if (!ck(h, cudaGraphInstantiate(&h->gexec, g, 0), "instantiate")) return CZ_ECUDA;
+        } else {
+            rc = CZ_OK;
+        }
+        cudaEventRecord(h->ev[0], h->st);
+        if (!ck(h, cudaGraphLaunch(h->gexec, h->st), "graph launch")) return CZ_ECUDA;
+        cudaEventRecord(h->ev[6], h->st);
+        if (!ck(h, cudaStreamSynchronize(h->st), "replay")) return CZ_ECUDA;
+        cudaEventElapsedTime(&s.ms_device, h->ev[0], h->ev[6]);
+        launches = h->last.kernels;
+    } else {
+        if ((rc = enqueue(h, true, launches))) return rc;
+        if (!ck(h, cudaStreamSynchronize(h->st), "replay")) return CZ_ECUDA;
+        read_times(h, &s);
+    }
+    s.kernels = launches;
+    s.n_primes = h->n; s.n_dense = h->ndense; s.n_sparse = h->nsparse; s.n_profiles = h->nprof;
+    // results must still pass every status check
+    h->hout.resize(h->nprof);
+    if (h->nprof) cudaMemcpy(h->hout.data(), h->b_out.p, sizeof(OutRecord) * h->nprof, cudaMemcpyDeviceToHost);
+    if ((rc = check_records(h, nullptr))) return rc;
+    if (stats) *stats = s;
+    return CZ_OK;
+}
+
+int cz_a4(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t *a4_out) {
+    if (!h || !primes || !a4_out) return CZ_EINVAL;
+    std::vector<u32> cnt(n);
+    // reuse the census path with an all-dense plan restricted to A4
+    cudaSetDevice(h->dev);
+    h->err.clear();
+    std::vector<PrimeDesc> hp(n);
+    for (u32 i = 0; i < n; ++i) {
+        if (primes[i] < 2u) { h->err = "prime out of domain"; return CZ_EINVAL; }
+        hp[i] = PrimeDesc{};
+        hp[i].p = primes[i];
+    }
+    if (!ensure(h, h->b_primes, sizeof(PrimeDesc) * n) || !ensure(h, h->b_a4, 4ull * n) || !ensure(h, h->b_counter, 64))
+        return CZ_ECUDA;
+    cudaMemcpyAsync(h->b_primes.p, hp.data(), sizeof(PrimeDesc) * n, cudaMemcpyHostToDevice, h->st);
+    cudaMemsetAsync(h->b_counter.p, 0, 64, h->st);
+    a4_kernel<<<(n + A4_WARPS - 1) / A4_WARPS, A4_WARPS * 32, 0, h->st>>>(P<PrimeDesc>(h->b_primes), n,
+                                                                      P<u32>(h->b_a4), P<u32>(h->b_counter) + 8);
+    cudaMemcpyAsync(a4_out, h->b_a4.p, 4ull * n, cudaMemcpyDeviceToHost, h->st);
+    u32 err = 0;
+    cudaMemcpyAsync(&err, P<u32>(h->b_counter) + 8, 4, cudaMemcpyDeviceToHost, h->st);
+    if (!ck(h, cudaStreamSynchronize(h->st), "a4")) return CZ_ECUDA;
+    if (err) { h->err = "refused: A4 point count not certified"; return CZ_EREFUSED; }
+    h->have_plan = false;
+    return CZ_OK;
+}
+
+// ---- reference-compatible adapter -------------------------------------------
+static cz_handle *g_base = nullptr;
+
+void baseline_init(unsigned cap) {
+    (void)cap;
+    if (!g_base) cz_open(nullptr, &g_base);
+}
+
+int baseline_profile(unsigned p, unsigned mask, unsigned *out, unsigned *prefix, int full) {
+    (void)full;
+    if (!g_base) baseline_init(0);
+    if (!g_base || p < 3u) return 2;
+    const u32 adm = mask_of(p);
+    if (mask & ~adm) return 2;
+    std::vector<cz_profile> rec(popc(adm));
+    u32 pp = p;
+    if (cz_census(g_base, &pp, 1, CZ_AUTO, rec.data(), (u32)rec.size(), nullptr, nullptr)) return 2;
+    for (const cz_profile &v : rec)
+        if (mask & (1u << (v.r - 2))) { out[v.r] = v.M; prefix[v.r] = v.L; }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+// common.cuh -- shared types and 32-bit Montgomery arithmetic for the
+// B200 (sm_100a) census kernels.
+//
+// Montgomery product with R = 2^32 for an odd modulus p < 2^32
+// (the reference's kit::mont, src/census/engine32/src/mont32.hpp:9-10):
+//   a*b*R^-1 mod p, formed from the two high products and the carry of the
+//   low half (lo(t) + lo(m p) == 0 mod 2^32, so the carry is lo(t) != 0).
+//   Four integer multiplies (mul.lo, mul.hi, mul.lo, mul.hi) per product.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+typedef uint32_t u32;
+typedef uint64_t u64;
+typedef int64_t i64;
+typedef int32_t i32;
+
+#define CZ_HD __host__ __device__ __forceinline__
+
+namespace cz {
+
+struct Mont {
+    u32 p;      // odd modulus
+    u32 ninv;   // -p^-1 mod 2^32
+    u32 one;    // R mod p
+    u32 r2;     // R^2 mod p
+};
+
+CZ_HD u32 neg_inverse32(u32 p) {
+    u32 x = p;                      // p*p == 1 mod 8
+    for (int i = 0; i < 5; ++i) x *= 2u - p * x;
+    return 0u - x;
+}
+
+CZ_HD Mont make_mont(u32 p) {
+    Mont m;
+    m.p = p;
+    m.ninv = neg_inverse32(p);
+    u64 R = (u64(1) << 32) % p;
+    m.one = (u32)R;
+    m.r2 = (u32)((R * R) % p);
+    return m;
+}
+
+#ifdef __CUDA_ARCH__
+CZ_HD u32 umulhi(u32 a, u32 b) { return __umulhi(a, b); }
+#else
+CZ_HD u32 umulhi(u32 a, u32 b) { return (u32)(((u64)a * b) >> 32); }
+#endif
+
+// a*b*2^-32 mod p for a, b < p
+CZ_HD u32 mmul(u32 a, u32 b, u32 p, u32 ninv) {
+    u32 tlo = a * b;
+    u32 thi = umulhi(a, b);
+    u32 m = tlo * ninv;
+    u32 mhi = umulhi(m, p);
+    u64 u = (u64)thi + mhi + (tlo != 0u);
+    return u >= p ? (u32)(u - p) : (u32)u;
+}
+
+CZ_HD u32 mmul(u32 a, u32 b, const Mont &M) { return mmul(a, b, M.p, M.ninv); }
+CZ_HD u32 to_mont(u32 x, const Mont &M) { return mmul(x, M.r2, M); }
+CZ_HD u32 from_mont(u32 x, const Mont &M) { return mmul(x, 1u, M); }
+
+// left-to-right binary power of a Montgomery residue
+CZ_HD u32 mpow(u32 a, u32 e, const Mont &M) {
+    if (e == 0) return M.one;
+    int top = 31;
+#ifdef __CUDA_ARCH__
+    top = 31 - __clz(e);
+#else
+    while (!((e >> top) & 1u)) --top;
+#endif
+    u32 v = a;
+    for (int i = top - 1; i >= 0; --i) {
+        v = mmul(v, v, M);
+        if ((e >> i) & 1u) v = mmul(v, a, M);
+    }
+    return v;
+}
+
+// plain modular helpers (64-bit, host or device, setup only)
+CZ_HD u32 mulmod64(u32 a, u32 b, u32 p) { return (u32)(((u64)a * b) % p); }
+
+CZ_HD u32 gcd32(u32 a, u32 b) {
+    while (b) { u32 t = a % b; a = b; b = t; }
+    return a;
+}
+
+CZ_HD u32 lcm_of_mask(u32 mask) {
+    u32 m = 1;
+    for (u32 r = 2; r <= 9; ++r)
+        if (mask & (1u << (r - 2))) m = m / gcd32(m, r) * r;
+    return m;
+}
+
+CZ_HD u32 mask_of(u32 p) {
+    u32 m = 0;
+    for (u32 r = 2; r <= 9; ++r)
+        if ((p - 1u) % r == 0u) m |= 1u << (r - 2);
+    return m;
+}
+
+CZ_HD u32 planes_for(u32 r) { return r <= 2 ? 1u : r <= 4 ? 2u : r <= 8 ? 3u : 4u; }
+
+// packed reduction key: longer run first, then least canonical witness
+CZ_HD u64 pack_key(u32 len, u32 witness) { return ((u64)len << 32) | (u64)(0xFFFFFFFFu - witness); }
+CZ_HD u32 key_len(u64 k) { return (u32)(k >> 32); }
+CZ_HD u32 key_witness(u64 k) { return 0xFFFFFFFFu - (u32)k; }
+
+// ---- per-prime and per-profile descriptors shared by host and device ----
+
+struct PrimeDesc {
+    u32 p;
+    u32 mask;
+    u32 m;           // lcm of admissible r
+    u32 e;           // (p-1)/m
+    u32 ninv, one, r2;
+    u32 z;           // Montgomery form of an element of exact order m
+    u32 sigma;       // label of -1 modulo m (0 or m/2)
+    u32 B;           // signed table radius (sparse)
+    u32 K0;          // plane centre word: index of n is n + 32*K0 + 31
+    u32 nwords;      // words per plane
+    u32 first_prof;  // index of this prime's first profile
+    u32 nprof;
+    u32 route;       // 1 dense, 2 sparse
+    u32 status;      // error bits set by kernels
+};
+
+struct ProfDesc {
+    u32 prime;       // index into PrimeDesc
+    u32 r;
+    u32 np;          // bit planes
+    u32 Q;           // cover window cap
+    u32 D;           // cover denominators 1..D
+    u32 out_slot;    // index in the caller's output array
+    u64 plane_off;   // word offset of plane 0 in the plane pool
+    u32 omega[9];    // Montgomery omega^j, omega = z^(m/r), j < r
+    u32 local;       // index of the prime within its route's list
+};
+
+// device-written per-profile results
+struct ProfState {
+    unsigned long long best;  // packed key of the best completed run
+    u32 seed;                 // longest monochromatic stretch seen in [1, B]
+    u32 firstnz;              // least n >= 1 with colour != 0 (prefix + 1)
+    u32 rows_done;
+    u32 status;
+    unsigned long long words;       // filter words visited
+    unsigned long long completions; // exact completions run
+};
+
+enum : u32 {
+    ST_OK = 0,
+    ST_ROOT = 1u << 0,       // no element of exact order m found
+    ST_LABEL = 1u << 1,      // a power missed the root table
+    ST_SEED = 1u << 2,       // seed too short for a certified threshold
+    ST_PREFIX = 1u << 3,     // prefix ran past the table
+    ST_VERIFY = 1u << 4,     // direct-power certification failed
+    ST_A4 = 1u << 5,         // point count not certified
+    ST_QUEUE = 1u << 6,      // candidate buffer overflow
+    ST_COVER = 1u << 7,      // cover certificate out of domain
+};
+
+}  // namespace cz

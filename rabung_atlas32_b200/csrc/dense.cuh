@@ -1,0 +1,289 @@
+// dense.cuh -- exhaustive half-interval census scan (the dense oracle).
+//
+// Behaviour follows the reference's dense oracle (src/census/dense_oracle.cu:12-66)
+// and historical dense engine (src/census/engine32/build/original_scan_gpu.cu:311-389):
+// colour every x in [1, (p-1)/2] by x^((p-1)/m) mod p (one power per x, shared
+// by all admissible r of p), keep per-segment run summaries, merge them in
+// order, and recover the full profile by reflection with an explicit centre
+// join.  The B200 design is its own: integer Montgomery powers (no FP64),
+// root labels from a shared-memory hash, run boundaries from warp ballots and
+// per-lane __clz on the change mask, segment summaries reduced per CTA in
+// shared memory and merged per profile on the device.
+//
+// Within [1, (p-1)/2] the canonical witness min(s, p-(s+len-1)) of a run
+// equals its start s, and the centre run (when r | (p-1)/2) has witness equal
+// to its start as well, so summaries carry starts.
+#pragma once
+#include "labels.cuh"
+
+namespace cz {
+
+constexpr int DENSE_WARPS = 8;           // warps per CTA = segments per chunk
+constexpr int DENSE_STEPS = 256;         // 32-wide steps per segment
+constexpr u32 DENSE_SEG = 32u * DENSE_STEPS;
+
+// ordered run summary of a contiguous interval [start, start+len)
+struct Summ {
+    u32 start, len;
+    u32 pre, suf;        // length of the run touching the left / right end
+    u32 best, bstart;    // longest run touching neither end, least start
+    u32 cf, cl;          // first / last colour
+};
+
+__device__ __forceinline__ void take_best(u32 &bl, u32 &bs, u32 l, u32 s) {
+    if (l > bl || (l == bl && l != 0 && s < bs)) { bl = l; bs = s; }
+}
+
+// a (left) then b (right)
+__device__ __forceinline__ Summ merge_summ(const Summ &a, const Summ &b) {
+    Summ o;
+    o.start = a.start;
+    o.len = a.len + b.len;
+    o.cf = a.cf;
+    o.cl = b.cl;
+    bool join = a.cl == b.cf;
+    o.pre = (join && a.pre == a.len) ? a.len + b.pre : a.pre;
+    o.suf = (join && b.suf == b.len) ? b.len + a.suf : b.suf;
+    o.best = a.best; o.bstart = a.bstart;
+    take_best(o.best, o.bstart, b.best, b.bstart);
+    bool a_closed_left = a.suf < a.len;   // a's suffix run does not touch a's left end
+    bool b_closed_right = b.pre < b.len;
+    if (join) {
+        if (a_closed_left && b_closed_right)
+            take_best(o.best, o.bstart, a.suf + b.pre, a.start + a.len - a.suf);
+    } else {
+        if (a_closed_left) take_best(o.best, o.bstart, a.suf, a.start + a.len - a.suf);
+        if (b_closed_right) take_best(o.best, o.bstart, b.pre, b.start);
+    }
+    return o;
+}
+
+struct DenseArgs {
+    const PrimeDesc *primes;       // all primes of the call
+    const u32 *dense_idx;          // dense-local index -> prime index
+    const ProfDesc *profs;
+    const u32 *chunk_prefix;       // [nprimes+1] CTA chunks per prime (prefix)
+    const u32 *summ_prefix;        // [nprimes] first chunk-summary slot of the prime
+    u32 nprimes;
+    u32 nchunks;                   // total chunks
+    Summ *summ;                    // per prime: nprof x nchunks chunk summaries, profile-major
+    ProfState *state;
+};
+
+// One CTA per (prime, chunk of DENSE_WARPS segments); one warp per segment.
+__global__ void __launch_bounds__(DENSE_WARPS * 32)
+dense_scan_kernel(DenseArgs a) {
+    extern __shared__ u32 dsm[];
+    __shared__ Summ wsum[DENSE_WARPS][8];
+    __shared__ u32 cur_prime;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    u32 prev_prime = 0xFFFFFFFFu;
+    u32 *keys = dsm;
+    unsigned short *labs = nullptr;
+    u32 slots = 0;
+    for (u32 chunk = blockIdx.x; chunk < a.nchunks; chunk += gridDim.x) {
+        if (threadIdx.x == 0) {
+            u32 lo = 0, hi = a.nprimes;           // last i with prefix[i] <= chunk
+            while (hi - lo > 1) {
+                u32 mid = (lo + hi) >> 1;
+                if (a.chunk_prefix[mid] <= chunk) lo = mid; else hi = mid;
+            }
+            cur_prime = lo;
+        }
+        __syncthreads();
+        const u32 pi = cur_prime;
+        const PrimeDesc P = a.primes[a.dense_idx[pi]];
+        const Mont M{P.p, P.ninv, P.one, P.r2};
+        if (pi != prev_prime) {
+            slots = hash_slots(P.m);
+            labs = reinterpret_cast<unsigned short *>(keys + slots);
+            build_root_hash(keys, labs, slots, M, P.z, P.m);
+            prev_prime = pi;
+        }
+        const u32 local_chunk = chunk - a.chunk_prefix[pi];
+        const u32 nh = (P.p - 1u) >> 1;
+        const u32 seg = local_chunk * DENSE_WARPS + warp;
+        const u32 seg_start = 1u + seg * DENSE_SEG;          // x of the first element
+        const u32 nprof = P.nprof;
+        // per-profile warp-uniform state
+        u32 rr[8], mg[8], carry_c[8], carry_start[8], carry_len[8], pre[8], bl[8], bs[8], cf[8];
+        bool inpre[8];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            u32 r = s < (int)nprof ? a.profs[P.first_prof + s].r : 2u;
+            rr[s] = r; mg[s] = magic_of(r);
+            carry_c[s] = 0xFFFFFFFFu; carry_start[s] = seg_start; carry_len[s] = 0;
+            pre[s] = 0; bl[s] = 0; bs[s] = 0; cf[s] = 0; inpre[s] = true;
+        }
+        u32 lastc[8];
+        bool active = seg_start <= nh;
+        u32 seg_end = active ? min(nh, seg_start + DENSE_SEG - 1u) : 0u;   // inclusive
+        u32 bad = 0;
+        if (active) {
+            const u32 nsteps = (seg_end - seg_start) / 32u + 1u;
+            for (u32 st = 0; st < nsteps; ++st) {
+                const u32 base = seg_start + st * 32u;
+                const u32 x = base + lane;
+                const bool valid = x <= seg_end;
+                const u32 nvalid = min(32u, seg_end - base + 1u);
+                u32 label = 0;
+                if (valid) {
+                    u32 y = mpow(to_mont(x, M), P.e, M);
+                    label = lookup_label(keys, labs, slots, y);
+                    if (label == 0xFFFFu) { bad = 1; label = 0; }
+                }
+#pragma unroll
+                for (int s = 0; s < 8; ++s) {
+                    if (s >= (int)nprof) break;
+                    const u32 c = mod_small(label, rr[s], mg[s]);
+                    u32 pc = __shfl_up_sync(0xFFFFFFFFu, c, 1);
+                    if (lane == 0) pc = carry_c[s];
+                    const bool chg = valid && (c != pc);
+                    const u32 C = __ballot_sync(0xFFFFFFFFu, chg);
+                    if (st == 0) cf[s] = __shfl_sync(0xFFFFFFFFu, c, 0);
+                    // run closing at lane-1 for each lane that starts a new run
+                    u32 clen = 0, cst = 0;
+                    if (chg) {
+                        const u32 below = C & ((1u << lane) - 1u);
+                        if (below) {
+                            const u32 h = 31u - __clz(below);
+                            clen = lane - h; cst = base + h;
+                        } else {
+                            clen = carry_len[s] + lane; cst = carry_start[s];
+                        }
+                    }
+                    // the first closed run of the segment is its prefix run
+                    if (inpre[s] && C) {
+                        const u32 first = __ffs(C) - 1u;   // lowest change lane
+                        const u32 plen = __shfl_sync(0xFFFFFFFFu, clen, first);
+                        if (plen > 0) {
+                            pre[s] = plen;
+                            inpre[s] = false;
+                            if (lane == (int)first) clen = 0;
+                        } else {
+                            // change at the segment's first element: the empty carry run
+                            const u32 rest = C & ~(1u << first);
+                            if (rest) {
+                                const u32 f2 = __ffs(rest) - 1u;
+                                const u32 pl2 = __shfl_sync(0xFFFFFFFFu, clen, f2);
+                                pre[s] = pl2;
+                                inpre[s] = false;
+                                if (lane == (int)f2) clen = 0;
+                            }
+                        }
+                    }
+                    const u32 mlen = __reduce_max_sync(0xFFFFFFFFu, clen);
+                    if (mlen > 0 && mlen >= bl[s]) {
+                        const u32 mst = __reduce_min_sync(0xFFFFFFFFu, clen == mlen ? cst : 0xFFFFFFFFu);
+                        take_best(bl[s], bs[s], mlen, mst);
+                    }
+                    if (C) {
+                        const u32 h = 31u - __clz(C);
+                        carry_start[s] = base + h;
+                        carry_len[s] = nvalid - h;
+                    } else {
+                        carry_len[s] += nvalid;
+                    }
+                    carry_c[s] = __shfl_sync(0xFFFFFFFFu, c, nvalid - 1u);
+                    lastc[s] = carry_c[s];
+                }
+            }
+        }
+        bad = __reduce_or_sync(0xFFFFFFFFu, bad);
+        if (lane == 0) {
+            if (bad) atomicOr(&a.state[P.first_prof].status, ST_LABEL);
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                if (s >= (int)nprof) break;
+                Summ o;
+                if (active) {
+                    o.start = seg_start; o.len = seg_end - seg_start + 1u;
+                    o.suf = carry_len[s];
+                    o.pre = inpre[s] ? o.len : pre[s];
+                    o.best = bl[s]; o.bstart = bs[s];
+                    o.cf = cf[s]; o.cl = lastc[s];
+                } else {
+                    o.start = 0; o.len = 0; o.pre = o.suf = o.best = o.bstart = 0; o.cf = o.cl = 0;
+                }
+                wsum[warp][s] = o;
+            }
+        }
+        __syncthreads();
+        // thread s merges the CTA's segments for profile s, in order
+        if (threadIdx.x < nprof) {
+            const int s = threadIdx.x;
+            Summ acc = wsum[0][s];
+            for (int w = 1; w < DENSE_WARPS; ++w)
+                if (wsum[w][s].len) acc = merge_summ(acc, wsum[w][s]);
+            const u32 nch = a.chunk_prefix[pi + 1] - a.chunk_prefix[pi];
+            a.summ[a.summ_prefix[pi] + (u32)s * nch + local_chunk] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+struct DenseMergeArgs {
+    const PrimeDesc *primes;
+    const ProfDesc *profs;
+    const u32 *chunk_prefix;
+    const u32 *summ_prefix;
+    u32 nprimes;
+    const Summ *summ;
+    ProfState *state;        // indexed by global profile index
+    u32 *prefix_out;         // L per global profile index
+};
+
+// one warp per dense profile: lanes merge contiguous runs of chunk summaries,
+// lane 0 merges the 32 partial summaries, applies the reflection centre join.
+__global__ void dense_merge_kernel(DenseMergeArgs a, const u32 *dense_prof_list, u32 ndprof) {
+    const u32 gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= ndprof) return;
+    const u32 gprof = dense_prof_list[gw];
+    const ProfDesc D = a.profs[gprof];
+    const u32 pi = D.local;                  // dense-local prime index
+    const PrimeDesc P = a.primes[D.prime];
+    const u32 s = gprof - P.first_prof;
+    const u32 nch = a.chunk_prefix[pi + 1] - a.chunk_prefix[pi];
+    const Summ *base = a.summ + a.summ_prefix[pi] + s * nch;
+    const u32 per = (nch + 31u) / 32u;
+    const u32 lo = min(nch, lane * per), hi = min(nch, lo + per);
+    Summ acc{};
+    bool have = false;
+    for (u32 i = lo; i < hi; ++i) {
+        Summ v = base[i];
+        if (!v.len) continue;
+        acc = have ? merge_summ(acc, v) : v;
+        have = true;
+    }
+    __shared__ Summ part[32 * 8];
+    Summ *mine = part + (threadIdx.x >> 5) * 32;
+    mine[lane] = have ? acc : Summ{};
+    __syncwarp();
+    if (lane != 0) return;
+    Summ tot{};
+    bool h2 = false;
+    for (int l = 0; l < 32; ++l) {
+        if (!mine[l].len) continue;
+        tot = h2 ? merge_summ(tot, mine[l]) : mine[l];
+        h2 = true;
+    }
+    const u32 p = P.p, nh = (p - 1u) >> 1, r = D.r;
+    const bool sym = (nh % r) == 0u;     // r | (p-1)/2: colour(p-x) = colour(x)
+    u32 bl = tot.best, bs = tot.bstart;
+    u32 L;
+    if (tot.pre == nh) {
+        // the whole half interval is one run
+        if (sym) { bl = p - 1u; bs = 1u; L = p - 1u; }
+        else { bl = nh; bs = 1u; L = nh; }
+    } else {
+        take_best(bl, bs, tot.pre, 1u);                       // run from x = 1
+        if (sym) take_best(bl, bs, 2u * tot.suf, nh - tot.suf + 1u);   // centre join
+        else take_best(bl, bs, tot.suf, nh - tot.suf + 1u);
+        L = tot.pre;                                          // colour(1) = 0
+    }
+    a.state[gprof].best = pack_key(bl, bs);
+    a.prefix_out[gprof] = L;
+}
+
+}  // namespace cz

@@ -1,0 +1,132 @@
+// finalize.cuh -- per-prime setup and per-profile finalisation kernels.
+//
+// setup_kernel: Montgomery constants, deterministic primality (the worker's
+// "worker primality" check, src/census/worker32.cu:18), a root z of exact order
+// m = lcm(r) (frozen_entry.cu:18-24), the label of -1, and the r-th roots of
+// unity omega^j = z^(j m / r) used by direct colour evaluation.
+//
+// finalize_kernel: M and witness from the packed key, L by direct powers from
+// x = 2 (the reference's prefix verification, worker32.cu:38), optional direct
+// certification of the witness run (certify_witness, B2/src/advance.cpp:7-13),
+// K by the scientific contract (docs/METHODS.md:11-18) and the output record.
+#pragma once
+#include "labels.cuh"
+
+namespace cz {
+
+// deterministic Miller-Rabin for n < 2^32 with bases 2, 3, 5, 7, 11 (no strong
+// pseudoprime to all five below 2.15e12)
+__device__ inline bool is_prime32(u32 n) {
+    if (n < 2u) return false;
+    const u32 bases[5] = {2, 3, 5, 7, 11};
+    for (int i = 0; i < 5; ++i) {
+        if (n == bases[i]) return true;
+        if (n % bases[i] == 0u) return false;
+    }
+    const Mont M = make_mont(n);
+    u32 d = n - 1u, s = 0;
+    while (!(d & 1u)) { d >>= 1; ++s; }
+    const u32 mone = n - M.one;           // Montgomery form of -1
+    for (int i = 0; i < 5; ++i) {
+        u32 x = mpow(to_mont(bases[i], M), d, M);
+        if (x == M.one || x == mone) continue;
+        bool pass = false;
+        for (u32 j = 1; j < s; ++j) {
+            x = mmul(x, x, M);
+            if (x == mone) { pass = true; break; }
+            if (x == M.one) return false;
+        }
+        if (!pass) return false;
+    }
+    return true;
+}
+
+__global__ void setup_kernel(PrimeDesc *primes, ProfDesc *profs, ProfState *state, u32 n) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    PrimeDesc P = primes[i];
+    u32 status = 0;
+    if (!is_prime32(P.p)) status |= ST_ROOT;
+    if (P.p > 2u) {
+        const Mont M = make_mont(P.p);
+        P.ninv = M.ninv; P.one = M.one; P.r2 = M.r2;
+        if (P.m > 1u) {
+            P.z = find_root_of_order(M, P.p, P.m, P.e);
+            if (!P.z) status |= ST_ROOT;
+        } else {
+            P.z = M.one;
+        }
+        P.sigma = (P.e & 1u) ? P.m / 2u : 0u;
+        for (u32 s = 0; s < P.nprof; ++s) {
+            ProfDesc &D = profs[P.first_prof + s];
+            const u32 w = mpow(P.z, P.m / D.r, M);
+            u32 v = M.one;
+            for (u32 j = 0; j < 9; ++j) {
+                D.omega[j] = j < D.r ? v : 0u;
+                v = mmul(v, w, M);
+            }
+            ProfState &S = state[P.first_prof + s];
+            S.best = 0; S.seed = 0; S.firstnz = 0xFFFFFFFFu; S.rows_done = 0;
+            S.status = 0; S.words = 0; S.completions = 0;
+        }
+    }
+    P.status = status;
+    primes[i] = P;
+}
+
+struct OutRecord {      // mirrors cz_profile in include/rabung_census.h
+    u32 p, r, M, L, witness, status;
+    unsigned long long K;
+};
+
+__device__ __forceinline__ u32 colour_pow(u32 x, const Mont &M, u32 ex, const u32 *om, u32 r) {
+    const u32 y = mpow(to_mont(x, M), ex, M);
+    for (u32 j = 0; j < r; ++j)
+        if (om[j] == y) return j;
+    return 0xFFFFFFFFu;
+}
+
+__global__ void finalize_kernel(const PrimeDesc *primes, const ProfDesc *profs, const ProfState *state,
+                                const u32 *dense_prefix, u32 nprof, u32 verify, OutRecord *out) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nprof) return;
+    const ProfDesc D = profs[g];
+    const PrimeDesc P = primes[D.prime];
+    const ProfState S = state[g];
+    const Mont M{P.p, P.ninv, P.one, P.r2};
+    const u32 p = P.p, r = D.r, ex = (p - 1u) / r;
+    u32 status = P.status | S.status;
+    const u32 Mlen = key_len(S.best), w = key_witness(S.best);
+    if (S.best == 0ull) status |= ST_VERIFY;
+    u32 L;
+    if (P.route == 1u) {
+        L = dense_prefix[g];
+    } else {
+        L = 1;                                   // colour(1) = 0
+        while (L + 1u < p && colour_pow(L + 1u, M, ex, D.omega, r) == 0u) {
+            ++L;
+            if (L > 4096u) { status |= ST_PREFIX; break; }
+        }
+    }
+    if (verify && !(status & (ST_ROOT | ST_LABEL)) && Mlen > 0u && Mlen <= 4096u) {
+        // the run [w, w+M-1] (or its mirror) is monochromatic and maximal
+        const u32 c0 = colour_pow(w, M, ex, D.omega, r);
+        bool ok = c0 != 0xFFFFFFFFu && (u64)w + Mlen - 1u <= p - 1u;
+        for (u32 k = 1; ok && k < Mlen; ++k) ok = colour_pow(w + k, M, ex, D.omega, r) == c0;
+        if (ok && w > 1u) ok = colour_pow(w - 1u, M, ex, D.omega, r) != c0;
+        if (ok && (u64)w + Mlen <= p - 1u) ok = colour_pow(w + Mlen, M, ex, D.omega, r) != c0;
+        u32 pl = 1;                              // prefix re-check from the scan result
+        if (ok && P.route == 1u) {
+            while (pl + 1u < p && pl <= L && colour_pow(pl + 1u, M, ex, D.omega, r) == 0u) ++pl;
+            ok = pl == L;
+        }
+        if (!ok) status |= ST_VERIFY;
+    }
+    OutRecord o;
+    o.p = p; o.r = r; o.M = Mlen; o.L = L; o.witness = w; o.status = status;
+    const u64 b = ((((u64)p - 1u) / 2u) % r == 0u) ? 2ull * L + 2ull : (u64)L + 2ull;
+    o.K = (u64)Mlen + 1ull > b ? (u64)Mlen + 1ull : b;
+    out[D.out_slot] = o;
+}
+
+}  // namespace cz

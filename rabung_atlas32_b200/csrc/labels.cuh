@@ -1,0 +1,77 @@
+// labels.cuh -- discrete-log labels of m-th roots of unity.
+//
+// For a prime p and m = lcm of the admissible orders r (m | p-1, m <= 2520),
+// x^((p-1)/m) is an m-th root of unity z^j for a fixed z of exact order m;
+// j is the label of x and colour_r(x) = j mod r (the reference's
+// character_root + sorted root table, src/census/engine32/src/frozen_entry.cu:18-24,
+// 158-167).  Here the m roots live in a shared-memory open-addressing hash
+// keyed by their Montgomery value, so a lookup is ~1-2 probes instead of a
+// 12-step binary search.
+#pragma once
+#include "common.cuh"
+
+namespace cz {
+
+// smallest power-of-two slot count >= 2m (m <= 2520 -> <= 8192 slots)
+CZ_HD u32 hash_slots(u32 m) {
+    u32 s = 8;
+    while (s < 2 * m) s <<= 1;
+    return s;
+}
+
+CZ_HD u32 hash_slot(u32 key, u32 bits) { return (key * 0x9E3779B1u) >> (32 - bits); }
+
+// element of exact order m: z = a^((p-1)/m) with z^(m/q) != 1 for each prime
+// q | m (the reference's character_root; only m is factored).
+CZ_HD u32 find_root_of_order(const Mont &M, u32 p, u32 m, u32 e) {
+    if (m == 1) return M.one;
+    for (u32 a = 2; a < p && a < 100000u; ++a) {
+        u32 z = mpow(to_mont(a, M), e, M);
+        bool ok = true;
+        const u32 qs[4] = {2, 3, 5, 7};
+        for (int i = 0; i < 4; ++i)
+            if (m % qs[i] == 0 && mpow(z, m / qs[i], M) == M.one) { ok = false; break; }
+        if (ok) return z;
+    }
+    return 0;
+}
+
+// Block-cooperative build of the root hash for one prime in shared memory.
+// keys[] must hold hash_slots(m) u32, labels[] as many u16.  All threads of
+// the block call this; ends with __syncthreads().
+__device__ inline void build_root_hash(u32 *keys, unsigned short *labels, u32 slots,
+                                       const Mont &M, u32 z, u32 m) {
+    for (u32 i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = 0u;
+    __syncthreads();
+    u32 bits = 31 - __clz(slots);
+    for (u32 j = threadIdx.x; j < m; j += blockDim.x) {
+        u32 v = mpow(z, j, M);            // Montgomery z^j (never 0: a unit)
+        u32 h = hash_slot(v, bits);
+        for (u32 probe = 0; probe < slots; ++probe) {
+            u32 old = atomicCAS(&keys[h], 0u, v);
+            if (old == 0u) { labels[h] = (unsigned short)j; break; }
+            h = (h + 1) & (slots - 1);
+        }
+    }
+    __syncthreads();
+}
+
+// label of a Montgomery m-th root of unity; 0xFFFF on a miss
+__device__ __forceinline__ u32 lookup_label(const u32 *keys, const unsigned short *labels,
+                                            u32 slots, u32 v) {
+    u32 bits = 31 - __clz(slots);
+    u32 h = hash_slot(v, bits);
+    for (u32 probe = 0; probe < slots; ++probe) {
+        u32 k = keys[h];
+        if (k == v) return labels[h];
+        if (k == 0u) return 0xFFFFu;
+        h = (h + 1) & (slots - 1);
+    }
+    return 0xFFFFu;
+}
+
+// exact floor(x / r) for x < 2^16, r <= 9: multiply by ceil(2^32 / r)
+CZ_HD u32 magic_of(u32 r) { return (u32)(((u64(1) << 32) + r - 1) / r); }
+CZ_HD u32 mod_small(u32 x, u32 r, u32 magic) { return x - r * umulhi(x, magic); }
+
+}  // namespace cz

@@ -1,0 +1,37 @@
+"""C ABI: the library loads and exports every symbol include/rabung_census.h
+declares (no compute calls: runs without a GPU)."""
+import ctypes
+import re
+
+from conftest import ROOT
+
+
+def declared():
+    h = (ROOT / "include" / "rabung_census.h").read_text()
+    body = re.sub(r"/\*.*?\*/", "", h, flags=re.S)
+    return sorted(set(re.findall(r"\b(cz_[a-z0-9_]+|baseline_[a-z]+)\s*\(", body)))
+
+
+def test_header_symbols_exported():
+    from rabung_atlas32_b200 import build, _lib
+    build.build()
+    lib = ctypes.CDLL(str(build.LIB))
+    names = declared()
+    assert "cz_census" in names and "baseline_profile" in names
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) <= set(_lib.EXPORTS)
+
+
+def test_struct_layouts():
+    from rabung_atlas32_b200 import _lib
+    assert ctypes.sizeof(_lib.cz_profile) == 32
+    assert ctypes.sizeof(_lib.cz_config) == 4 * (1 + 1 + 1 + 10 + 1 + 1 + 1 + 1 + 6)
+
+
+def test_count_profiles_host_only():
+    from rabung_atlas32_b200 import _lib, codec
+    lib = _lib.load()
+    ps = [2, 3, 5, 7, 4294967291]
+    arr = (ctypes.c_uint32 * len(ps))(*ps)
+    assert lib.cz_count_profiles(arr, len(ps)) == sum(bin(codec.expected_mask(p)).count("1") for p in ps[1:])

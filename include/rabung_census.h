@@ -71,6 +71,7 @@ typedef struct cz_stats {
     uint32_t n_primes, n_dense, n_sparse, n_profiles, n_fallback;
     uint32_t kernels;               /* kernel launches of the call */
     uint64_t words, completions;    /* sparse filter words visited, exact completions */
+    uint64_t tests;                 /* plane-window comparisons executed by the filter */
     uint64_t h2d_bytes, d2h_bytes;
 } cz_stats;
 
@@ -102,6 +103,12 @@ int cz_replay(cz_handle *h, cz_stats *stats);
 /* Quadratic A4 counts only (src/census/moment_worker.cpp:19-52 semantics):
  * x in [1, p-4] with x..x+3 all of one quadratic character; 0 for p = 2. */
 int cz_a4(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t *a4_out);
+
+/* Measured integer peaks of this GPU (for the roofline; no reference
+ * counterpart): kind 0 = plane-word tests per second (one funnel shift plus
+ * one three-input logic op on 32-bit words), kind 1 = 32-bit Montgomery
+ * products per second. */
+int cz_microbench(cz_handle *h, uint32_t kind, double *per_second);
 
 /* Reference-compatible adapter (src/census/engine32/src/baseline_bridge.cu:7,21-27):
  * profile of one prime for the orders in `mask` (bit r-2), M into out[r] and

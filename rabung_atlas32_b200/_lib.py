@@ -34,14 +34,14 @@ class cz_stats(ctypes.Structure):
                 ("ms_device", ctypes.c_float), ("ms_h2d", ctypes.c_float), ("ms_d2h", ctypes.c_float),
                 ("n_primes", u32), ("n_dense", u32), ("n_sparse", u32), ("n_profiles", u32),
                 ("n_fallback", u32), ("kernels", u32), ("words", u64), ("completions", u64),
-                ("h2d_bytes", u64), ("d2h_bytes", u64)]
+                ("tests", u64), ("h2d_bytes", u64), ("d2h_bytes", u64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_count_profiles",
-           "cz_census", "cz_replay", "cz_a4", "baseline_init", "baseline_profile"]
+           "cz_census", "cz_replay", "cz_a4", "cz_microbench", "baseline_init", "baseline_profile"]
 
 _lib = None
 
@@ -73,6 +73,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.cz_replay.restype = ctypes.c_int
     L.cz_a4.argtypes = [H, ctypes.POINTER(u32), u32, ctypes.POINTER(u32)]
     L.cz_a4.restype = ctypes.c_int
+    L.cz_microbench.argtypes = [H, u32, ctypes.POINTER(ctypes.c_double)]
+    L.cz_microbench.restype = ctypes.c_int
     L.baseline_init.argtypes = [ctypes.c_uint]
     L.baseline_init.restype = None
     L.baseline_profile.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),

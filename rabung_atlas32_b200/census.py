@@ -123,6 +123,14 @@ class Census:
             raise CensusError(f"replay refused (rc={rc}): {self._err()}")
         return st.as_dict()
 
+    def microbench(self, kind: int) -> float:
+        """Measured peak: kind 0 plane-word tests/s, kind 1 Montgomery products/s."""
+        v = ctypes.c_double()
+        rc = self.lib.cz_microbench(self.h, kind, ctypes.byref(v))
+        if rc != 0:
+            raise CensusError(f"microbench failed (rc={rc}): {self._err()}")
+        return v.value
+
     def a4(self, primes) -> list:
         n = len(primes)
         arr = _as_u32_array(primes)

@@ -25,6 +25,7 @@
 #include "sparse.cuh"
 #include "finalize.cuh"
 #include "a4.cuh"
+#include "microbench.cuh"
 #include "../../include/rabung_census.h"
 
 using namespace cz;
@@ -105,6 +106,8 @@ struct cz_handle {
     cudaGraphExec_t gexec = nullptr;
     cz_stats last{};
     std::vector<OutRecord> hout;
+    void *pin = nullptr;
+    size_t pin_cap = 0;
 };
 
 namespace {
@@ -295,10 +298,24 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
 
 int upload(cz_handle *h, cz_stats *s) {
     cudaStream_t st = h->st;
+    size_t total = sizeof(PrimeDesc) * h->n + sizeof(ProfDesc) * h->nprof +
+                   4ull * (h->h_chunk.size() + h->h_summp.size() + h->ndense + h->nsparse + h->nsl + h->ndl) + 64 * 8;
+    if (h->pin_cap < total) {
+        if (h->pin) cudaFreeHost(h->pin);
+        h->pin = nullptr;
+        h->pin_cap = 0;
+        if (!ck(h, cudaHostAlloc(&h->pin, total + total / 4, cudaHostAllocDefault), "cudaHostAlloc")) return CZ_ECUDA;
+        h->pin_cap = total + total / 4;
+    }
+    // the host plan is staged in pinned memory and copied asynchronously
+    char *stage = static_cast<char *>(h->pin);
     size_t bytes = 0;
     auto put = [&](Buf &b, const void *src, size_t n) {
-        bytes += n;
-        return n == 0 || ck(h, cudaMemcpyAsync(b.p, src, n, cudaMemcpyHostToDevice, st), "h2d");
+        if (n == 0) return true;
+        std::memcpy(stage + bytes, src, n);
+        const bool ok = ck(h, cudaMemcpyAsync(b.p, stage + bytes, n, cudaMemcpyHostToDevice, st), "h2d");
+        bytes += (n + 63) & ~size_t(63);
+        return ok;
     };
     if (!put(h->b_primes, h->hp.data(), sizeof(PrimeDesc) * h->n) ||
         !put(h->b_profs, h->hprof.data(), sizeof(ProfDesc) * h->nprof) ||
@@ -481,6 +498,7 @@ void cz_close(cz_handle *h) {
                    &h->b_summp, &h->b_didx, &h->b_sidx, &h->b_slist, &h->b_dlist, &h->b_dpre, &h->b_out,
                    &h->b_a4, &h->b_counter};
     for (Buf *b : bufs) if (b->p) cudaFree(b->p);
+    if (h->pin) cudaFreeHost(h->pin);
     if (h->d_small) cudaFree(h->d_small);
     if (h->d_chain) cudaFree(h->d_chain);
     for (auto &e : h->ev) if (e) cudaEventDestroy(e);
@@ -539,7 +557,7 @@ static int census_impl(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_
     {
         std::vector<ProfState> hs(h->nprof);
         if (h->nprof) cudaMemcpy(hs.data(), h->b_state.p, sizeof(ProfState) * h->nprof, cudaMemcpyDeviceToHost);
-        for (auto &x : hs) { s.words += x.words; s.completions += x.completions; }
+        for (auto &x : hs) { s.words += x.words; s.completions += x.completions; s.tests += x.tests; }
     }
     if (flags & CZ_A4) {
         u32 a4err = 0;
@@ -647,6 +665,28 @@ int cz_a4(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t *a4_out) {
     if (!ck(h, cudaStreamSynchronize(h->st), "a4")) return CZ_ECUDA;
     if (err) { h->err = "refused: A4 point count not certified"; return CZ_EREFUSED; }
     h->have_plan = false;
+    return CZ_OK;
+}
+
+int cz_microbench(cz_handle *h, uint32_t kind, double *per_second) {
+    if (!h || !per_second || kind > 1) return CZ_EINVAL;
+    cudaSetDevice(h->dev);
+    if (!ensure(h, h->b_counter, 64)) return CZ_ECUDA;
+    const u32 blocks = (u32)h->sms * 8u, threads = 256, iters = kind == 0 ? 4096u : 1024u;
+    const u32 p = 4294967291u;
+    const Mont M = make_mont(p);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(h->ev[0], h->st);
+        if (kind == 0) mb_alu_kernel<<<blocks, threads, 0, h->st>>>(iters, 0x9E3779B9u + rep, P<u32>(h->b_counter));
+        else mb_mont_kernel<<<blocks, threads, 0, h->st>>>(iters, p, M.ninv, P<u32>(h->b_counter));
+        cudaEventRecord(h->ev[1], h->st);
+        if (!ck(h, cudaStreamSynchronize(h->st), "microbench")) return CZ_ECUDA;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+        if (rep > 0 && ms < best) best = ms;
+    }
+    *per_second = (double)blocks * threads * iters * 8.0 / (best * 1e-3);
     return CZ_OK;
 }
 

@@ -148,6 +148,7 @@ struct ProfState {
     u32 status;
     unsigned long long words;       // filter words visited
     unsigned long long completions; // exact completions run
+    unsigned long long tests;       // plane-window comparisons (stage x plane) executed
 };
 
 enum : u32 {

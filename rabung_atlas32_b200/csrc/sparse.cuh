@@ -102,7 +102,7 @@ struct ProfCtx {
 
 // exact completion of one candidate; returns packed key (0 on reject) and
 // sets *err on an arithmetic failure
-__device__ u64 complete_one(const ProfCtx &c, u32 b, u32 d, u32 dinv, u32 *err) {
+__device__ __noinline__ u64 complete_one(const ProfCtx &c, u32 b, u32 d, u32 dinv, u32 *err) {
     const u32 p = c.p;
     const u32 xr = mmul(b, dinv, c.M);                 // b * d^-1 mod p (dinv in Montgomery form)
     if (xr == 0u) return 0;
@@ -140,10 +140,58 @@ __device__ u64 complete_one(const ProfCtx &c, u32 b, u32 d, u32 dinv, u32 *err) 
     return pack_key(len, w);
 }
 
-__global__ void __launch_bounds__(SPARSE_WARPS * 32)
+// window of plane k at bit index u (planes are NW words apart)
+__device__ __forceinline__ u32 winp(const u32 *__restrict__ P, u32 k, u32 NW, u32 u) {
+    return win(P + (size_t)k * NW, u);
+}
+
+// bilateral screen of one word: keep bits whose run can still reach Ts
+// (right matches + left matches >= Ts - t); unknown numerators match
+__device__ __noinline__ u32 screen_word(const ProfCtx &c, const u32 *base_w, u32 b0, u32 alive, u32 d, u32 t, u32 h) {
+    if (h >= 64u) return alive;
+    const u32 u0 = b0 + c.OFF;
+    u32 R[64];
+    u32 cur = alive;
+    bool unk = false;
+    R[0] = cur;
+    for (u32 k3 = 1; k3 <= h; ++k3) {
+        if (cur && !unk) {
+            const i64 lim = (i64)c.B - (i64)b0 - (i64)k3 * d;        // bits i <= lim known
+            if (lim < 0) unk = true;
+            else {
+                const u32 u = u0 + k3 * d;
+                u32 eq = 0xFFFFFFFFu;
+                for (u32 k2 = 0; k2 < c.np; ++k2) eq &= ~(winp(c.P, k2, c.NW, u) ^ base_w[k2]);
+                const u32 known = lim >= 31 ? 0xFFFFFFFFu : ((2u << (u32)lim) - 1u);
+                cur &= eq | ~known;
+            }
+        }
+        R[k3] = cur;
+    }
+    u32 lcur = alive, kept = R[h] & alive;
+    bool lunk = false;
+    for (u32 k3 = 1; k3 <= h && (lcur & ~kept); ++k3) {
+        if (!lunk) {
+            const i64 low = (i64)(t - 1u + k3) * d - (i64)c.B - (i64)b0;   // bits i >= low known
+            if (low >= 32) lunk = true;
+            else {
+                const u32 u = u0 - (t - 1u + k3) * d;
+                u32 eq = 0xFFFFFFFFu;
+                for (u32 k2 = 0; k2 < c.np; ++k2) eq &= ~(winp(c.P, k2, c.NW, u) ^ base_w[k2]);
+                const u32 known = low <= 0 ? 0xFFFFFFFFu : ~((1u << (u32)low) - 1u);
+                lcur &= eq | ~known;
+            }
+        }
+        kept |= R[h - k3] & lcur;
+    }
+    return kept;
+}
+
+__global__ void __launch_bounds__(SPARSE_WARPS * 32, 2)
 sparse_kernel(SparseArgs a) {
     __shared__ u32 s_item, s_row;
-    __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];
+    __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];      // candidates awaiting completion
+    __shared__ uint2 sbuf[SPARSE_WARPS][CAND_CAP];     // (b0, alive) words awaiting the screen
     __shared__ u32 s_err;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (;;) {
@@ -166,13 +214,16 @@ sparse_kernel(SparseArgs a) {
         c.P = a.planes + PD.plane_off;
 #pragma unroll
         for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
+        const u32 *P0 = c.P, *P1 = c.P + c.NW, *P2 = c.P + 2u * (size_t)c.NW, *P3 = c.P + 3u * (size_t)c.NW;
+        const u32 np = c.np;
         const u32 seed = *(volatile u32 *)&st->seed;
         const u32 tpref = anchor_pref(c.r, a.tune.anchor_bits);
-        u32 ncand = 0;                       // warp-uniform buffer fill
+        u32 ncand = 0, nscr = 0;             // warp-uniform buffer fills
         u64 warp_best = 0;
         u32 words = 0, comps = 0, err = 0;
+        u32 tests = 0;
+        // complete `count` (<= 32) buffered candidates, one per lane
         auto flush = [&](u32 count) {
-            // complete count (<= 32) buffered candidates, one per lane
             u64 key = 0;
             if ((u32)lane < count) {
                 const Cand cd = cbuf[warp][lane];
@@ -181,19 +232,13 @@ sparse_kernel(SparseArgs a) {
                 err |= e;
             }
             comps += count;
-            // warp max of 64-bit keys
-            u32 hi = (u32)(key >> 32);
+            const u32 hi = (u32)(key >> 32);
             const u32 mhi = __reduce_max_sync(0xFFFFFFFFu, hi);
             const u32 lo = __reduce_max_sync(0xFFFFFFFFu, hi == mhi ? (u32)key : 0u);
             const u64 k2 = ((u64)mhi << 32) | lo;
             if (k2 > warp_best) warp_best = k2;
             __syncwarp();
-            // shift the remainder down
-            if (ncand > count) {
-                const u32 rest = ncand - count;
-                if ((u32)lane < rest) cbuf[warp][lane] = cbuf[warp][count + lane];
-                // (rest <= 32 because the buffer holds < 64 entries)
-            }
+            if (ncand > count && (u32)lane < ncand - count) cbuf[warp][lane] = cbuf[warp][count + lane];
             __syncwarp();
             ncand -= count;
             if (lane == 0 && warp_best) atomicMax(&st->best, (unsigned long long)warp_best);
@@ -203,14 +248,14 @@ sparse_kernel(SparseArgs a) {
             if (lane == 0) d = atomicAdd(&s_row, 1u);
             d = __shfl_sync(0xFFFFFFFFu, d, 0);
             if (d > c.D) break;
-            // per-row parameters from the verified maximum so far
+            // row parameters from the verified maximum so far (<= M)
             const u64 bk = *(volatile unsigned long long *)&st->best;
-            const u32 blen = key_len(bk) > seed ? key_len(bk) : seed;   // <= M
+            const u32 blen = key_len(bk) > seed ? key_len(bk) : seed;
             const u32 q = blen < c.Q ? blen : c.Q;
-            if (q < 3u) { err = 1; break; }
+            if (q < 3u) { err |= 2u; break; }
             const u32 t = tpref < q ? (tpref < 2u ? 2u : tpref) : q;
             const u32 s = q - t + 1u;
-            const u32 Ts = blen;                 // screen: reject runs certified < blen
+            const u32 h = blen > t ? blen - t : 0u;      // screen: reject runs certified < blen
             const u32 beta = ((t - 1u) * d + 1u) >> 1;
             if (beta > c.B) continue;
             const u32 ds = d * s;
@@ -218,83 +263,29 @@ sparse_kernel(SparseArgs a) {
             const u32 nw = (d + 31u) >> 5;
             const u32 W = K * nw;
             const float rnw = 1.0f / (float)nw;
-            u32 dinv = 0;                        // lazily: Montgomery d^-1
+            u32 dinv = 0;
             bool have_inv = false;
-            for (u32 base = 0; base < W; base += 32u) {
-                const u32 rank = base + (u32)lane;
+            // screen the queued words (count <= 32), push survivors to the completion buffer
+            auto screen_batch = [&](u32 count) {
                 u32 keep = 0, b0 = 0;
-                if (rank < W) {
-                    u32 k = (u32)((float)rank * rnw);
-                    if (k * nw > rank) --k;
-                    else if ((k + 1u) * nw <= rank) ++k;
-                    const u32 w = rank - k * nw;
-                    b0 = beta + k * ds + 32u * w;
-                    u32 len = d - 32u * w;
-                    if (len > 32u) len = 32u;
-                    if (b0 > c.B) len = 0;
-                    else if (c.B - b0 + 1u < len) len = c.B - b0 + 1u;
-                    u32 alive = len >= 32u ? 0xFFFFFFFFu : ((1u << len) - 1u);
-                    const u32 u0 = b0 + c.OFF;
-                    if (alive) {
-                        ++words;
-                        u32 base_w[4];
-#pragma unroll
-                        for (int k2 = 0; k2 < 4; ++k2)
-                            base_w[k2] = (k2 < (int)c.np) ? win(c.P + (size_t)k2 * c.NW, u0) : 0u;
-                        for (u32 j = 1; j < t && alive; ++j) {
-                            const u32 u = u0 - j * d;
-#pragma unroll
-                            for (int k2 = 0; k2 < 4; ++k2)
-                                if (k2 < (int)c.np) alive &= ~(win(c.P + (size_t)k2 * c.NW, u) ^ base_w[k2]);
-                        }
-                        if (alive && a.tune.screen && Ts > t && Ts - t < 64u) {
-                            // bilateral screen: keep iff (right matches) + (left matches) >= Ts - t,
-                            // unknown numerators (outside [-B, B]) counting as matches
-                            const u32 h = Ts - t;
-                            u32 R[64];
-                            u32 cur = alive;
-                            bool unk = false;
-                            R[0] = cur;
-                            for (u32 k3 = 1; k3 <= h; ++k3) {
-                                if (cur && !unk) {
-                                    const i64 lim = (i64)c.B - (i64)b0 - (i64)k3 * d;   // bits i <= lim known
-                                    if (lim < 0) unk = true;
-                                    else {
-                                        const u32 u = u0 + k3 * d;
-                                        u32 eq = 0xFFFFFFFFu;
-#pragma unroll
-                                        for (int k2 = 0; k2 < 4; ++k2)
-                                            if (k2 < (int)c.np) eq &= ~(win(c.P + (size_t)k2 * c.NW, u) ^ base_w[k2]);
-                                        const u32 known = lim >= 31 ? 0xFFFFFFFFu : ((2u << (u32)lim) - 1u);
-                                        cur &= eq | ~known;
-                                    }
-                                }
-                                R[k3] = cur;
-                            }
-                            u32 lcur = alive, kept = R[h] & alive;
-                            bool lunk = false;
-                            for (u32 k3 = 1; k3 <= h; ++k3) {
-                                if (lcur && !lunk) {
-                                    const i64 low = (i64)(t - 1u + k3) * d - (i64)c.B - (i64)b0;  // bits i >= low known
-                                    if (low >= 32) lunk = true;
-                                    else {
-                                        const u32 u = u0 - (t - 1u + k3) * d;
-                                        u32 eq = 0xFFFFFFFFu;
-#pragma unroll
-                                        for (int k2 = 0; k2 < 4; ++k2)
-                                            if (k2 < (int)c.np) eq &= ~(win(c.P + (size_t)k2 * c.NW, u) ^ base_w[k2]);
-                                        const u32 known = low <= 0 ? 0xFFFFFFFFu : ~((1u << (u32)low) - 1u);
-                                        lcur &= eq | ~known;
-                                    }
-                                }
-                                kept |= R[h - k3] & lcur;
-                            }
-                            alive = kept;
-                        }
-                        keep = alive;
+                if ((u32)lane < count) {
+                    const uint2 e = sbuf[warp][lane];
+                    b0 = e.x;
+                    keep = e.y;
+                    if (a.tune.screen && h > 0u) {
+                        const u32 u0 = b0 + c.OFF;
+                        u32 bw[4];
+                        bw[0] = win(P0, u0);
+                        bw[1] = np > 1u ? win(P1, u0) : 0u;
+                        bw[2] = np > 2u ? win(P2, u0) : 0u;
+                        bw[3] = np > 3u ? win(P3, u0) : 0u;
+                        keep = screen_word(c, bw, b0, keep, d, t, h);
                     }
                 }
-                // drain survivors into the warp buffer, one bit per lane per round
+                __syncwarp();
+                if (nscr > count && (u32)lane < nscr - count) sbuf[warp][lane] = sbuf[warp][count + lane];
+                __syncwarp();
+                nscr -= count;
                 while (__any_sync(0xFFFFFFFFu, keep != 0u)) {
                     if (!have_inv) {
                         // Montgomery d^-1 (= R d^-1), so mmul(b, dinv) = b d^-1 mod p
@@ -313,18 +304,64 @@ sparse_kernel(SparseArgs a) {
                     __syncwarp();
                     if (ncand >= 32u) flush(32u);
                 }
+            };
+            for (u32 base = 0; base < W; base += 32u) {
+                const u32 rank = base + (u32)lane;
+                u32 alive = 0, b0 = 0;
+                if (rank < W) {
+                    u32 k = (u32)((float)rank * rnw);
+                    if (k * nw > rank) --k;
+                    else if ((k + 1u) * nw <= rank) ++k;
+                    const u32 w = rank - k * nw;
+                    b0 = beta + k * ds + 32u * w;
+                    u32 len = d - 32u * w;
+                    if (len > 32u) len = 32u;
+                    if (b0 > c.B) len = 0;
+                    else if (c.B - b0 + 1u < len) len = c.B - b0 + 1u;
+                    alive = len >= 32u ? 0xFFFFFFFFu : ((1u << len) - 1u);
+                }
+                if (alive) {
+                    ++words;
+                    u32 u = b0 + c.OFF;
+                    const u32 w0 = win(P0, u);
+                    const u32 w1 = np > 1u ? win(P1, u) : 0u;
+                    const u32 w2 = np > 2u ? win(P2, u) : 0u;
+                    const u32 w3 = np > 3u ? win(P3, u) : 0u;
+                    tests += np;                           // base windows
+                    for (u32 j = 1; j < t && alive; ++j) {
+                        tests += np;
+                        u -= d;
+                        u32 m = win(P0, u) ^ w0;
+                        if (np > 1u) m |= win(P1, u) ^ w1;
+                        if (np > 2u) m |= win(P2, u) ^ w2;
+                        if (np > 3u) m |= win(P3, u) ^ w3;
+                        alive &= ~m;
+                    }
+                }
+                // queue surviving words for the batched screen
+                const bool has = alive != 0u;
+                const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
+                if (bal) {
+                    const u32 pos = __popc(bal & ((1u << lane) - 1u));
+                    if (has) sbuf[warp][nscr + pos] = make_uint2(b0, alive);
+                    nscr += __popc(bal);
+                    __syncwarp();
+                    if (nscr >= 32u) screen_batch(32u);
+                }
             }
+            if (nscr) screen_batch(nscr);
         }
         if (ncand) flush(ncand);
-        if (err) atomicOr(&s_err, 1u);
-        // counters
+        if (err) atomicOr(&s_err, err);
         words = __reduce_add_sync(0xFFFFFFFFu, words);
+        tests = __reduce_add_sync(0xFFFFFFFFu, tests);
         if (lane == 0) {
             atomicAdd(&st->words, (unsigned long long)words);
             atomicAdd(&st->completions, (unsigned long long)comps);
+            atomicAdd(&st->tests, (unsigned long long)tests);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && s_err) atomicOr(&st->status, ST_QUEUE);
+        if (threadIdx.x == 0 && s_err) atomicOr(&st->status, (s_err & 2u) ? ST_SEED : ST_QUEUE);
     }
 }
 

@@ -34,6 +34,7 @@ namespace {
 
 constexpr u32 CHAIN_LIMIT = (1u << 20) + 8192u;   // table labels cover n < CHAIN_LIMIT
 constexpr u32 B_MAX = (1u << 20);
+constexpr u32 TABLE_DYN_SMEM = 190u * 1024u;        // dynamic part; static part ~34 KB
 
 struct Buf {
     void *p = nullptr;
@@ -211,6 +212,8 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
             P.B = B;
             P.K0 = (B + 31u) / 32u + 4u;
             P.nwords = 2u * P.K0 + 8u;
+            P.K2 = (B + 63u) / 64u + 4u;
+            P.nwords2 = 2u * P.K2 + 8u;
             h->h_sidx.push_back(i);
             max_slots_t = std::max(max_slots_t, hash_slots(P.m));
         } else {
@@ -230,12 +233,13 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
             D.prime = i;
             D.r = r;
             D.np = planes_for(r);
+            D.npp = planes_stored(r);
             D.out_slot = (u32)h->hprof.size();
             if (sparse) {
                 D.Q = q_for(c, r);
                 D.D = Ds[k];
-                D.plane_off = plane_words;
-                plane_words += (u64)D.np * P.nwords;
+                D.plane_off = plane_words;              // multiple of 4 words: vector loads align
+                plane_words += ((u64)D.npp * (P.nwords + P.nwords2) + 3ull) & ~3ull;
                 D.local = (u32)h->h_sidx.size() - 1u;
                 h->h_slist.push_back((u32)h->hprof.size());
             } else {
@@ -273,6 +277,10 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
         max_nq = (u32)(std::lower_bound(hs.begin(), hs.end(), nmax) - hs.begin());
     }
     h->table_smem = max_slots_t * 6u + 8u + max_nq * 2u + 16u;
+    if (h->table_smem > TABLE_DYN_SMEM) {
+        h->err = "table shared memory above the per-block limit";
+        return CZ_EINVAL;
+    }
     h->dense_smem = max_slots_d * 6u + 16u;
     // device buffers
     if (!ensure(h, h->b_primes, sizeof(PrimeDesc) * n) ||
@@ -482,7 +490,7 @@ int cz_open(const cz_config *cfg, cz_handle **out) {
     h->sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) { delete h; return CZ_ECUDA; }
     for (auto &e : h->ev) cudaEventCreate(&e);
-    cudaFuncSetAttribute(table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_DYN_SMEM);
     cudaFuncSetAttribute(dense_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     if (!build_static_tables(h)) { cz_close(h); return CZ_ECUDA; }
     *out = h;

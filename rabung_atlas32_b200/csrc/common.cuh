@@ -102,6 +102,7 @@ CZ_HD u32 mask_of(u32 p) {
 }
 
 CZ_HD u32 planes_for(u32 r) { return r <= 2 ? 1u : r <= 4 ? 2u : r <= 8 ? 3u : 4u; }
+CZ_HD u32 planes_stored(u32 r) { return r <= 2 ? 1u : r <= 4 ? 2u : 4u; }
 
 // packed reduction key: longer run first, then least canonical witness
 CZ_HD u64 pack_key(u32 len, u32 witness) { return ((u64)len << 32) | (u64)(0xFFFFFFFFu - witness); }
@@ -119,8 +120,10 @@ struct PrimeDesc {
     u32 z;           // Montgomery form of an element of exact order m
     u32 sigma;       // label of -1 modulo m (0 or m/2)
     u32 B;           // signed table radius (sparse)
-    u32 K0;          // plane centre word: index of n is n + 32*K0 + 31
-    u32 nwords;      // words per plane
+    u32 K0;          // base view: index of n is n + 32*K0 + 31
+    u32 nwords;      // base view words per plane
+    u32 K2;          // odd view: index of n = 2i+1 is i + 32*K2
+    u32 nwords2;     // odd view words per plane
     u32 first_prof;  // index of this prime's first profile
     u32 nprof;
     u32 route;       // 1 dense, 2 sparse
@@ -131,6 +134,7 @@ struct ProfDesc {
     u32 prime;       // index into PrimeDesc
     u32 r;
     u32 np;          // bit planes
+    u32 npp;         // planes as stored (np padded to 1, 2 or 4), interleaved
     u32 Q;           // cover window cap
     u32 D;           // cover denominators 1..D
     u32 out_slot;    // index in the caller's output array

@@ -12,10 +12,10 @@
 
 namespace cz {
 
-// smallest power-of-two slot count >= 2m (m <= 2520 -> <= 8192 slots)
+// smallest power-of-two slot count >= 3m/2 (m <= 2520 -> <= 4096 slots)
 CZ_HD u32 hash_slots(u32 m) {
     u32 s = 8;
-    while (s < 2 * m) s <<= 1;
+    while (2 * s < 3 * m) s <<= 1;
     return s;
 }
 

@@ -3,24 +3,26 @@
 // Mathematics (the reference's GPU method, paper/GPU_METHOD_EN.tex:256-560):
 //  * Cover (Thm "integer coverage certificate"; P/src/clipped_cover.hpp:7-21):
 //    with H = Q-1, B < p, D < p, H*D <= 2B and 4BD - H D^2 > 4p, every window
-//    x..x+H of [1, p-1] has numerators a+jd (a = dx mod p, 1 <= d <= D) all in
-//    [-B, B]; colour(x+j) = colour(a+jd) - colour(d), so colour constancy of
-//    the window is read off the signed table.
+//    x..x+H of [1, p-1] has numerators a+jd (a = dx mod p, 1 <= d <= D,
+//    gcd(a, d) = 1) all in [-B, B]; colour(x+j) = colour(a+jd) - colour(d), so
+//    colour constancy of the window is read off the signed table.
 //  * A run of length >= q (q <= Q) contains a q-window; it holds s = q-t+1
 //    anchors of length t along its row.  Writing an anchor by its top
 //    numerator b (numerators b, b-d, ..., b-(t-1)d) and v = b - ceil((t-1)d/2),
 //    this build selects b iff v mod (d*s) < d: every s consecutive anchors of a
 //    row contain exactly one selected b, and the rule is symmetric under the
 //    reflection b -> (t-1)d - b (colours shift by colour(-1), positions x ->
-//    p-x, canonical witness unchanged), so only v >= 0 is enumerated
-//    (the role of the reference's folded bands and phase rule,
-//    P/src/periodic_bands.hpp:28-78; this rule keeps whole bands of d
-//    consecutive b, so each 32-bit word is full).
+//    p-x, canonical witness unchanged), so only v >= 0 is enumerated (the role
+//    of the reference's folded bands and phase rule, P/src/periodic_bands.hpp:28-78;
+//    this rule keeps whole bands of d consecutive b, so 32-bit words are full).
+//    The anchors of a primitive row share gcd(b, d) = 1, so for even d only odd
+//    b are enumerated, on the odd-numerator view of the table (the reference's
+//    G = 2 wheel, PBV/src/wheel_filter.hpp:14-46).
 //  * Filter (PBV/src/wheel_filter.hpp:52-91): 32 anchors per word; a candidate
 //    survives while every anchor offset agrees with b on every colour plane.
 //  * Bilateral screen (B1/src/two_cuts.hpp:27-74): reject only when known
-//    mismatches on both sides bound the run below the threshold; numerators
-//    outside [-B, B] are unknown and never reject.
+//    mismatches on both sides bound the run below the verified maximum;
+//    numerators outside [-B, B] are unknown and never reject.
 //  * Exact completion (PBV/src/completion.hpp:17-57, E32/src/completion_core.hpp:17-48):
 //    x = b/d mod p, extend both ways with table colours, falling back to a
 //    direct power outside the table; reduce by (length, least witness) with a
@@ -33,17 +35,18 @@
 // (its planes stay hot in that SM's L1 and in L2), its warps pull rows d in
 // increasing order from a shared-memory counter and re-read the verified
 // maximum at every row, so the threshold rises while the profile runs; lanes
-// take consecutive words of a row (coalesced plane reads, funnel-shift
-// windows); survivors go to a per-warp shared-memory buffer and are completed
-// 32 at a time, one per lane.
+// take consecutive words of a row (one vector load fetches all interleaved
+// planes of a word, funnel shifts cut the windows); words that survive the
+// anchor are queued per warp and screened 32 at a time, one per lane, and the
+// screened candidates are completed 32 at a time, one per lane.
 #pragma once
 #include "labels.cuh"
 
 namespace cz {
 
 constexpr int SPARSE_WARPS = 16;
-constexpr int CAND_CAP = 64;          // per-warp candidate buffer
-constexpr u32 RUN_CAP = 4096;         // longest run a completion may walk (M <= 46 below 2^32 in practice)
+constexpr int CAND_CAP = 64;          // per-warp buffers
+constexpr u32 RUN_CAP = 4096;         // longest run a completion may walk
 
 struct Tuning {
     u32 anchor_bits;   // t chosen so 32 * r^-(t-1) <= 2^-anchor_bits per word
@@ -63,11 +66,6 @@ struct SparseArgs {
 
 struct Cand { u32 b, d, dinv; };
 
-__device__ __forceinline__ u32 win(const u32 *__restrict__ P, u32 u) {
-    const u32 w = u >> 5;
-    return __funnelshift_r(__ldg(P + w), __ldg(P + w + 1), u & 31u);
-}
-
 // preferred anchor length: least t with r^(t-1) >= 2^(5+bits), i.e. a word of
 // 32 random anchors keeps on average <= 2^-bits survivors
 __device__ __forceinline__ u32 anchor_pref(u32 r, u32 bits) {
@@ -78,27 +76,76 @@ __device__ __forceinline__ u32 anchor_pref(u32 r, u32 bits) {
     return k + 1u;
 }
 
-// colour of numerator n (|n| <= B) as an integer, np planes of NW words
-__device__ __forceinline__ u32 colour_at(const u32 *__restrict__ P, u32 NW, u32 np, u32 u) {
-    u32 c = 0;
-    for (u32 k = 0; k < np; ++k) c |= ((__ldg(P + (size_t)k * NW + (u >> 5)) >> (u & 31u)) & 1u) << k;
-    return c;
+// windows of all NPP interleaved planes at bit index u
+template <int NPP> struct Planes;
+template <> struct Planes<1> {
+    static __device__ __forceinline__ void win(const u32 *__restrict__ P, u32 u, u32 *o) {
+        const u32 *q = P + (u >> 5);
+        o[0] = __funnelshift_r(__ldg(q), __ldg(q + 1), u & 31u);
+    }
+};
+template <> struct Planes<2> {
+    static __device__ __forceinline__ void win(const u32 *__restrict__ P, u32 u, u32 *o) {
+        const uint2 *q = reinterpret_cast<const uint2 *>(P) + (u >> 5);
+        const uint2 a = __ldg(q), b = __ldg(q + 1);
+        o[0] = __funnelshift_r(a.x, b.x, u & 31u);
+        o[1] = __funnelshift_r(a.y, b.y, u & 31u);
+    }
+};
+template <> struct Planes<4> {
+    static __device__ __forceinline__ void win(const u32 *__restrict__ P, u32 u, u32 *o) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(P) + (u >> 5);
+        const uint4 a = __ldg(q), b = __ldg(q + 1);
+        const u32 sh = u & 31u;
+        o[0] = __funnelshift_r(a.x, b.x, sh);
+        o[1] = __funnelshift_r(a.y, b.y, sh);
+        o[2] = __funnelshift_r(a.z, b.z, sh);
+        o[3] = __funnelshift_r(a.w, b.w, sh);
+    }
+};
+
+// mismatch mask of a window against the base windows
+template <int NPP>
+__device__ __forceinline__ u32 mismatch(const u32 *__restrict__ P, u32 u, const u32 *base) {
+    u32 w[NPP];
+    Planes<NPP>::win(P, u, w);
+    u32 m = w[0] ^ base[0];
+#pragma unroll
+    for (int k = 1; k < NPP; ++k) m |= w[k] ^ base[k];
+    return m;
+}
+
+// one view of the signed table: index i <-> numerator c + G i, i in [ilo, ihi]
+struct View {
+    const u32 *P;     // interleaved planes
+    u32 OFF;          // bit index of i = 0
+    i32 ilo, ihi;
+    u32 G, c;
+};
+
+struct ProfCtx {
+    u32 p, r, np, npp, Q, D, B, NW, OFF, ex;
+    Mont M;
+    const u32 *P;          // base view planes
+    View base, odd;
+    u32 om[9];
+};
+
+// colour of numerator n (|n| <= B) as an integer, from the base view
+__device__ __forceinline__ u32 colour_at(const ProfCtx &c, u32 u) {
+    const u32 *q = c.P + (size_t)(u >> 5) * c.npp;
+    u32 col = 0;
+    for (u32 k = 0; k < c.np; ++k) col |= ((__ldg(q + k) >> (u & 31u)) & 1u) << k;
+    return col;
 }
 
 // absolute colour of x in [1, p-1] by a direct power: x^((p-1)/r) = omega^j
-__device__ __forceinline__ u32 colour_direct(u32 x, const Mont &M, u32 ex, const u32 *om, u32 r) {
-    const u32 y = mpow(to_mont(x, M), ex, M);
-    for (u32 j = 0; j < r; ++j)
-        if (om[j] == y) return j;
+__device__ __forceinline__ u32 colour_direct(u32 x, const ProfCtx &c) {
+    const u32 y = mpow(to_mont(x, c.M), c.ex, c.M);
+    for (u32 j = 0; j < c.r; ++j)
+        if (c.om[j] == y) return j;
     return 0xFFFFFFFFu;
 }
-
-struct ProfCtx {
-    u32 p, r, np, Q, D, B, NW, OFF, ex;
-    Mont M;
-    const u32 *P;          // plane 0
-    u32 om[9];
-};
 
 // exact completion of one candidate; returns packed key (0 on reject) and
 // sets *err on an arithmetic failure
@@ -106,143 +153,240 @@ __device__ __noinline__ u64 complete_one(const ProfCtx &c, u32 b, u32 d, u32 din
     const u32 p = c.p;
     const u32 xr = mmul(b, dinv, c.M);                 // b * d^-1 mod p (dinv in Montgomery form)
     if (xr == 0u) return 0;
-    const u32 cb = colour_at(c.P, c.NW, c.np, b + c.OFF);
-    const u32 cd = colour_at(c.P, c.NW, c.np, d + c.OFF);
+    const u32 cb = colour_at(c, b + c.OFF);
+    const u32 cd = colour_at(c, d + c.OFF);
     const u32 A = cb >= cd ? cb - cd : cb + c.r - cd;  // absolute colour of x_R
     u32 right = 0, left = 0;
-    // extend right: x = xr + k, numerator b + k d
-    for (u32 k = 1;; ++k) {
+    for (u32 k = 1;; ++k) {                            // x = xr + k, numerator b + k d
         if (k > RUN_CAP) { *err = 1; return 0; }
         const u64 x = (u64)xr + k;
         if (x >= p) break;
         const u64 n = (u64)b + (u64)k * d;
-        bool same;
-        if (n <= c.B) same = colour_at(c.P, c.NW, c.np, (u32)n + c.OFF) == cb;
-        else same = colour_direct((u32)x, c.M, c.ex, c.om, c.r) == A;
+        const bool same = n <= c.B ? colour_at(c, (u32)n + c.OFF) == cb : colour_direct((u32)x, c) == A;
         if (!same) break;
         right = k;
     }
-    // extend left: x = xr - k, numerator b - k d
-    for (u32 k = 1;; ++k) {
+    for (u32 k = 1;; ++k) {                            // x = xr - k, numerator b - k d
         if (k > RUN_CAP) { *err = 1; return 0; }
-        if (k >= xr) break;                            // x would reach 0
+        if (k >= xr) break;
         const u32 x = xr - k;
         const i64 n = (i64)b - (i64)k * d;
-        bool same;
-        if (n >= -(i64)c.B) same = colour_at(c.P, c.NW, c.np, (u32)(n + (i64)c.OFF)) == cb;
-        else same = colour_direct(x, c.M, c.ex, c.om, c.r) == A;
+        const bool same = n >= -(i64)c.B ? colour_at(c, (u32)(n + (i64)c.OFF)) == cb : colour_direct(x, c) == A;
         if (!same) break;
         left = k;
     }
     const u32 s = xr - left, e = xr + right;
-    const u32 len = e - s + 1u;
     const u32 w = s < p - e ? s : p - e;
-    return pack_key(len, w);
+    return pack_key(e - s + 1u, w);
 }
 
-// window of plane k at bit index u (planes are NW words apart)
-__device__ __forceinline__ u32 winp(const u32 *__restrict__ P, u32 k, u32 NW, u32 u) {
-    return win(P + (size_t)k * NW, u);
-}
-
-// bilateral screen of one word: keep bits whose run can still reach Ts
-// (right matches + left matches >= Ts - t); unknown numerators match
-__device__ __noinline__ u32 screen_word(const ProfCtx &c, const u32 *base_w, u32 b0, u32 alive, u32 d, u32 t, u32 h) {
+// bilateral screen of one word at view index i0 (row step dd = d / G): keep
+// bits whose run can still reach t + h (right matches + left matches >= h);
+// indices outside [ilo, ihi] are unknown and match
+template <int NPP>
+__device__ __noinline__ u32 screen_word(const View &v, u32 i0, u32 alive, u32 dd, u32 t, u32 h) {
     if (h >= 64u) return alive;
-    const u32 u0 = b0 + c.OFF;
+    const u32 u0 = i0 + v.OFF;
+    u32 base[NPP];
+    Planes<NPP>::win(v.P, u0, base);
     u32 R[64];
     u32 cur = alive;
     bool unk = false;
     R[0] = cur;
-    for (u32 k3 = 1; k3 <= h; ++k3) {
+    for (u32 k = 1; k <= h; ++k) {
         if (cur && !unk) {
-            const i64 lim = (i64)c.B - (i64)b0 - (i64)k3 * d;        // bits i <= lim known
+            const i64 lim = (i64)v.ihi - (i64)(i32)i0 - (i64)k * dd;     // bits <= lim known
             if (lim < 0) unk = true;
             else {
-                const u32 u = u0 + k3 * d;
-                u32 eq = 0xFFFFFFFFu;
-                for (u32 k2 = 0; k2 < c.np; ++k2) eq &= ~(winp(c.P, k2, c.NW, u) ^ base_w[k2]);
+                const u32 m = mismatch<NPP>(v.P, u0 + k * dd, base);
                 const u32 known = lim >= 31 ? 0xFFFFFFFFu : ((2u << (u32)lim) - 1u);
-                cur &= eq | ~known;
+                cur &= ~(m & known);
             }
         }
-        R[k3] = cur;
+        R[k] = cur;
     }
     u32 lcur = alive, kept = R[h] & alive;
     bool lunk = false;
-    for (u32 k3 = 1; k3 <= h && (lcur & ~kept); ++k3) {
+    for (u32 k = 1; k <= h && (lcur & ~kept); ++k) {
         if (!lunk) {
-            const i64 low = (i64)(t - 1u + k3) * d - (i64)c.B - (i64)b0;   // bits i >= low known
+            const i64 low = (i64)v.ilo - (i64)(i32)i0 + (i64)(t - 1u + k) * dd;   // bits >= low known
             if (low >= 32) lunk = true;
             else {
-                const u32 u = u0 - (t - 1u + k3) * d;
-                u32 eq = 0xFFFFFFFFu;
-                for (u32 k2 = 0; k2 < c.np; ++k2) eq &= ~(winp(c.P, k2, c.NW, u) ^ base_w[k2]);
+                const u32 m = mismatch<NPP>(v.P, u0 - (t - 1u + k) * dd, base);
                 const u32 known = low <= 0 ? 0xFFFFFFFFu : ~((1u << (u32)low) - 1u);
-                lcur &= eq | ~known;
+                lcur &= ~(m & known);
             }
         }
-        kept |= R[h - k3] & lcur;
+        kept |= R[h - k] & lcur;
     }
     return kept;
 }
 
+// warp state carried across rows of one profile
+struct WarpQ {
+    u32 ncand, nscr;
+    u64 best;
+    u32 words, comps, tests, err;
+};
+
+// complete `count` (<= 32) buffered candidates, one per lane
+__device__ __forceinline__ void flush_cands(const ProfCtx &c, Cand *cb, WarpQ &q, u32 count, ProfState *st, int lane) {
+    u64 key = 0;
+    if ((u32)lane < count) {
+        const Cand cd = cb[lane];
+        u32 e = 0;
+        key = complete_one(c, cd.b, cd.d, cd.dinv, &e);
+        q.err |= e;
+    }
+    q.comps += count;
+    const u32 hi = (u32)(key >> 32);
+    const u32 mhi = __reduce_max_sync(0xFFFFFFFFu, hi);
+    const u32 lo = __reduce_max_sync(0xFFFFFFFFu, hi == mhi ? (u32)key : 0u);
+    const u64 k2 = ((u64)mhi << 32) | lo;
+    if (k2 > q.best) q.best = k2;
+    __syncwarp();
+    if (q.ncand > count && (u32)lane < q.ncand - count) cb[lane] = cb[count + lane];
+    __syncwarp();
+    q.ncand -= count;
+    if (lane == 0 && q.best) atomicMax(&st->best, (unsigned long long)q.best);
+}
+
+// screen `count` (<= 32) queued words of the current row and queue the
+// surviving candidates for completion
+template <int NPP>
+__device__ __forceinline__ void screen_batch(const ProfCtx &c, const View &v, uint2 *sb, Cand *cb, WarpQ &q,
+                                             u32 count, u32 d, u32 dd, u32 t, u32 h, bool screen, u32 &dinv,
+                                             bool &have_inv, ProfState *st, int lane) {
+    u32 keep = 0, i0 = 0;
+    if ((u32)lane < count) {
+        const uint2 e = sb[lane];
+        i0 = e.x;
+        keep = e.y;
+        if (screen && h > 0u) keep = screen_word<NPP>(v, i0, keep, dd, t, h);
+    }
+    __syncwarp();
+    if (q.nscr > count && (u32)lane < q.nscr - count) sb[lane] = sb[count + lane];
+    __syncwarp();
+    q.nscr -= count;
+    while (__any_sync(0xFFFFFFFFu, keep != 0u)) {
+        if (!have_inv) {
+            // Montgomery d^-1 (= R d^-1), so mmul(b, dinv) = b d^-1 mod p
+            dinv = mpow(to_mont(d, c.M), c.p - 2u, c.M);
+            have_inv = true;
+        }
+        const bool has = keep != 0u;
+        const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
+        const u32 pos = __popc(bal & ((1u << lane) - 1u));
+        if (has) {
+            const u32 bit = __ffs(keep) - 1u;
+            keep &= keep - 1u;
+            cb[q.ncand + pos] = Cand{v.c + v.G * (i0 + bit), d, dinv};
+        }
+        q.ncand += __popc(bal);
+        __syncwarp();
+        if (q.ncand >= 32u) flush_cands(c, cb, q, 32u, st, lane);
+    }
+}
+
+// all selected words of row d on view v (anchor filter, queue, screen, complete)
+template <int NPP>
+__device__ __forceinline__ void filter_row(const ProfCtx &c, const View &vref, u32 d, u32 t, u32 s, u32 h,
+                                           const Tuning &tune, uint2 *sb, Cand *cb, WarpQ &q, ProfState *st,
+                                           int lane) {
+    const View v = vref;
+    const u32 G = v.G, dd = d / G;
+    const u32 beta = ((t - 1u) * d + 1u) >> 1;
+    // first view index of band 0: least i with c + G i >= beta
+    const i32 istart = (i32)((beta >= v.c ? beta - v.c + G - 1u : 0u) / G);
+    if (istart > v.ihi) return;
+    const u32 step = dd * s;                       // band period in view indices
+    const u32 K = (u32)(v.ihi - istart) / step + 1u;
+    const u32 nw = (dd + 31u) >> 5;
+    const u32 W = K * nw;
+    const float rnw = 1.0f / (float)nw;
+    u32 dinv = 0;
+    bool have_inv = false;
+    for (u32 base = 0; base < W; base += 32u) {
+        const u32 rank = base + (u32)lane;
+        u32 alive = 0, i0 = 0;
+        if (rank < W) {
+            u32 k = (u32)((float)rank * rnw);
+            if (k * nw > rank) --k;
+            else if ((k + 1u) * nw <= rank) ++k;
+            const u32 w = rank - k * nw;
+            i0 = (u32)istart + k * step + 32u * w;
+            u32 len = dd - 32u * w;
+            if (len > 32u) len = 32u;
+            if ((i32)i0 > v.ihi) len = 0;
+            else if ((u32)(v.ihi - (i32)i0) + 1u < len) len = (u32)(v.ihi - (i32)i0) + 1u;
+            alive = len >= 32u ? 0xFFFFFFFFu : ((1u << len) - 1u);
+        }
+        if (alive) {
+            ++q.words;
+            u32 u = i0 + v.OFF;
+            u32 bw[NPP];
+            Planes<NPP>::win(v.P, u, bw);
+            u32 j = 1;
+            for (; j < t && alive; ++j) {
+                u -= dd;
+                alive &= ~mismatch<NPP>(v.P, u, bw);
+            }
+            q.tests += j * (u32)NPP;
+        }
+        const bool has = alive != 0u;
+        const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
+        if (bal) {
+            const u32 pos = __popc(bal & ((1u << lane) - 1u));
+            if (has) sb[q.nscr + pos] = make_uint2(i0, alive);
+            q.nscr += __popc(bal);
+            __syncwarp();
+            if (q.nscr >= 32u)
+                screen_batch<NPP>(c, v, sb, cb, q, 32u, d, dd, t, h, tune.screen != 0u, dinv, have_inv, st, lane);
+        }
+    }
+    if (q.nscr)
+        screen_batch<NPP>(c, v, sb, cb, q, q.nscr, d, dd, t, h, tune.screen != 0u, dinv, have_inv, st, lane);
+}
+
 __global__ void __launch_bounds__(SPARSE_WARPS * 32, 2)
 sparse_kernel(SparseArgs a) {
-    __shared__ u32 s_item, s_row;
+    __shared__ u32 s_item, s_row, s_err;
     __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];      // candidates awaiting completion
-    __shared__ uint2 sbuf[SPARSE_WARPS][CAND_CAP];     // (b0, alive) words awaiting the screen
-    __shared__ u32 s_err;
+    __shared__ uint2 sbuf[SPARSE_WARPS][CAND_CAP];     // (index, alive) words awaiting the screen
+    __shared__ ProfCtx s_ctx;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (;;) {
         if (threadIdx.x == 0) {
             s_item = atomicAdd(a.next, 1u);
             s_row = 1u;
             s_err = 0u;
+            if (s_item < a.nlist) {
+                const u32 gprof = a.prof_list[s_item];
+                const ProfDesc PD = a.profs[gprof];
+                const PrimeDesc PR = a.primes[PD.prime];
+                ProfCtx c;
+                c.p = PR.p; c.r = PD.r; c.np = PD.np; c.npp = PD.npp; c.Q = PD.Q; c.D = PD.D; c.B = PR.B;
+                c.NW = PR.nwords; c.OFF = 32u * PR.K0 + 31u; c.ex = (PR.p - 1u) / PD.r;
+                c.M = Mont{PR.p, PR.ninv, PR.one, PR.r2};
+                c.P = a.planes + PD.plane_off;
+                c.base = View{c.P, c.OFF, -(i32)PR.B, (i32)PR.B, 1u, 0u};
+                // odd view: n = 2i + 1 in [-B, B]  <=>  i in [ceil((-B-1)/2), floor((B-1)/2)]
+                c.odd = View{c.P + (size_t)PR.nwords * PD.npp, 32u * PR.K2, -(i32)((PR.B + 1u) / 2u),
+                             (i32)((PR.B - 1u) / 2u), 2u, 1u};
+                for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
+                s_ctx = c;
+            }
         }
         __syncthreads();
         const u32 item = s_item;
         if (item >= a.nlist) return;
-        const u32 gprof = a.prof_list[item];
-        const ProfDesc PD = a.profs[gprof];
-        const PrimeDesc PR = a.primes[PD.prime];
-        ProfState *st = a.state + gprof;
-        ProfCtx c;
-        c.p = PR.p; c.r = PD.r; c.np = PD.np; c.Q = PD.Q; c.D = PD.D; c.B = PR.B;
-        c.NW = PR.nwords; c.OFF = 32u * PR.K0 + 31u; c.ex = (PR.p - 1u) / PD.r;
-        c.M = Mont{PR.p, PR.ninv, PR.one, PR.r2};
-        c.P = a.planes + PD.plane_off;
-#pragma unroll
-        for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
-        const u32 *P0 = c.P, *P1 = c.P + c.NW, *P2 = c.P + 2u * (size_t)c.NW, *P3 = c.P + 3u * (size_t)c.NW;
-        const u32 np = c.np;
+        const ProfCtx &c = s_ctx;
+        ProfState *st = a.state + a.prof_list[item];
         const u32 seed = *(volatile u32 *)&st->seed;
         const u32 tpref = anchor_pref(c.r, a.tune.anchor_bits);
-        u32 ncand = 0, nscr = 0;             // warp-uniform buffer fills
-        u64 warp_best = 0;
-        u32 words = 0, comps = 0, err = 0;
-        u32 tests = 0;
-        // complete `count` (<= 32) buffered candidates, one per lane
-        auto flush = [&](u32 count) {
-            u64 key = 0;
-            if ((u32)lane < count) {
-                const Cand cd = cbuf[warp][lane];
-                u32 e = 0;
-                key = complete_one(c, cd.b, cd.d, cd.dinv, &e);
-                err |= e;
-            }
-            comps += count;
-            const u32 hi = (u32)(key >> 32);
-            const u32 mhi = __reduce_max_sync(0xFFFFFFFFu, hi);
-            const u32 lo = __reduce_max_sync(0xFFFFFFFFu, hi == mhi ? (u32)key : 0u);
-            const u64 k2 = ((u64)mhi << 32) | lo;
-            if (k2 > warp_best) warp_best = k2;
-            __syncwarp();
-            if (ncand > count && (u32)lane < ncand - count) cbuf[warp][lane] = cbuf[warp][count + lane];
-            __syncwarp();
-            ncand -= count;
-            if (lane == 0 && warp_best) atomicMax(&st->best, (unsigned long long)warp_best);
-        };
+        WarpQ q{0, 0, 0, 0, 0, 0, 0};
+        uint2 *sb = sbuf[warp];
+        Cand *cb = cbuf[warp];
         for (;;) {
             u32 d = 0;
             if (lane == 0) d = atomicAdd(&s_row, 1u);
@@ -251,113 +395,23 @@ sparse_kernel(SparseArgs a) {
             // row parameters from the verified maximum so far (<= M)
             const u64 bk = *(volatile unsigned long long *)&st->best;
             const u32 blen = key_len(bk) > seed ? key_len(bk) : seed;
-            const u32 q = blen < c.Q ? blen : c.Q;
-            if (q < 3u) { err |= 2u; break; }
-            const u32 t = tpref < q ? (tpref < 2u ? 2u : tpref) : q;
-            const u32 s = q - t + 1u;
+            const u32 q_ = blen < c.Q ? blen : c.Q;
+            if (q_ < 3u) { q.err |= 2u; break; }
+            const u32 t = tpref < q_ ? (tpref < 2u ? 2u : tpref) : q_;
+            const u32 s = q_ - t + 1u;
             const u32 h = blen > t ? blen - t : 0u;      // screen: reject runs certified < blen
-            const u32 beta = ((t - 1u) * d + 1u) >> 1;
-            if (beta > c.B) continue;
-            const u32 ds = d * s;
-            const u32 K = (c.B - beta) / ds + 1u;
-            const u32 nw = (d + 31u) >> 5;
-            const u32 W = K * nw;
-            const float rnw = 1.0f / (float)nw;
-            u32 dinv = 0;
-            bool have_inv = false;
-            // screen the queued words (count <= 32), push survivors to the completion buffer
-            auto screen_batch = [&](u32 count) {
-                u32 keep = 0, b0 = 0;
-                if ((u32)lane < count) {
-                    const uint2 e = sbuf[warp][lane];
-                    b0 = e.x;
-                    keep = e.y;
-                    if (a.tune.screen && h > 0u) {
-                        const u32 u0 = b0 + c.OFF;
-                        u32 bw[4];
-                        bw[0] = win(P0, u0);
-                        bw[1] = np > 1u ? win(P1, u0) : 0u;
-                        bw[2] = np > 2u ? win(P2, u0) : 0u;
-                        bw[3] = np > 3u ? win(P3, u0) : 0u;
-                        keep = screen_word(c, bw, b0, keep, d, t, h);
-                    }
-                }
-                __syncwarp();
-                if (nscr > count && (u32)lane < nscr - count) sbuf[warp][lane] = sbuf[warp][count + lane];
-                __syncwarp();
-                nscr -= count;
-                while (__any_sync(0xFFFFFFFFu, keep != 0u)) {
-                    if (!have_inv) {
-                        // Montgomery d^-1 (= R d^-1), so mmul(b, dinv) = b d^-1 mod p
-                        dinv = mpow(to_mont(d, c.M), c.p - 2u, c.M);
-                        have_inv = true;
-                    }
-                    const bool has = keep != 0u;
-                    const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
-                    const u32 pos = __popc(bal & ((1u << lane) - 1u));
-                    if (has) {
-                        const u32 bit = __ffs(keep) - 1u;
-                        keep &= keep - 1u;
-                        cbuf[warp][ncand + pos] = Cand{b0 + bit, d, dinv};
-                    }
-                    ncand += __popc(bal);
-                    __syncwarp();
-                    if (ncand >= 32u) flush(32u);
-                }
-            };
-            for (u32 base = 0; base < W; base += 32u) {
-                const u32 rank = base + (u32)lane;
-                u32 alive = 0, b0 = 0;
-                if (rank < W) {
-                    u32 k = (u32)((float)rank * rnw);
-                    if (k * nw > rank) --k;
-                    else if ((k + 1u) * nw <= rank) ++k;
-                    const u32 w = rank - k * nw;
-                    b0 = beta + k * ds + 32u * w;
-                    u32 len = d - 32u * w;
-                    if (len > 32u) len = 32u;
-                    if (b0 > c.B) len = 0;
-                    else if (c.B - b0 + 1u < len) len = c.B - b0 + 1u;
-                    alive = len >= 32u ? 0xFFFFFFFFu : ((1u << len) - 1u);
-                }
-                if (alive) {
-                    ++words;
-                    u32 u = b0 + c.OFF;
-                    const u32 w0 = win(P0, u);
-                    const u32 w1 = np > 1u ? win(P1, u) : 0u;
-                    const u32 w2 = np > 2u ? win(P2, u) : 0u;
-                    const u32 w3 = np > 3u ? win(P3, u) : 0u;
-                    tests += np;                           // base windows
-                    for (u32 j = 1; j < t && alive; ++j) {
-                        tests += np;
-                        u -= d;
-                        u32 m = win(P0, u) ^ w0;
-                        if (np > 1u) m |= win(P1, u) ^ w1;
-                        if (np > 2u) m |= win(P2, u) ^ w2;
-                        if (np > 3u) m |= win(P3, u) ^ w3;
-                        alive &= ~m;
-                    }
-                }
-                // queue surviving words for the batched screen
-                const bool has = alive != 0u;
-                const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
-                if (bal) {
-                    const u32 pos = __popc(bal & ((1u << lane) - 1u));
-                    if (has) sbuf[warp][nscr + pos] = make_uint2(b0, alive);
-                    nscr += __popc(bal);
-                    __syncwarp();
-                    if (nscr >= 32u) screen_batch(32u);
-                }
-            }
-            if (nscr) screen_batch(nscr);
+            const View &v = (d & 1u) ? c.base : c.odd;
+            if (c.npp == 1u) filter_row<1>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
+            else if (c.npp == 2u) filter_row<2>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
+            else filter_row<4>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
         }
-        if (ncand) flush(ncand);
-        if (err) atomicOr(&s_err, err);
-        words = __reduce_add_sync(0xFFFFFFFFu, words);
-        tests = __reduce_add_sync(0xFFFFFFFFu, tests);
+        if (q.ncand) flush_cands(c, cb, q, q.ncand, st, lane);
+        if (q.err) atomicOr(&s_err, q.err);
+        const u32 words = __reduce_add_sync(0xFFFFFFFFu, q.words);
+        const u32 tests = __reduce_add_sync(0xFFFFFFFFu, q.tests);
         if (lane == 0) {
             atomicAdd(&st->words, (unsigned long long)words);
-            atomicAdd(&st->completions, (unsigned long long)comps);
+            atomicAdd(&st->completions, (unsigned long long)q.comps);
             atomicAdd(&st->tests, (unsigned long long)tests);
         }
         __syncthreads();

@@ -1,21 +1,32 @@
 // table.cuh -- signed colour bit-planes for the certified rational-anchor filter.
 //
 // For a sparse-routed prime p with table radius B, every admissible order r gets
-// np = ceil(log2 r) bit planes over the signed numerators n in [-B, B]:
-// the bit at index u = n + 32*K0 + 31 of plane k is bit k of colour_r(n) written
-// in binary, with colour_r(-n) = colour_r(n) + colour_r(-1).  This replaces the
-// reference's small_table / fine_labels / pack_pair kernels
-// (src/census/engine32/src/small_table.cuh:7-52) and its folded mirror rows.
+// bit planes of colour_r (written in binary, np = ceil(log2 r) planes, padded to
+// NPP in {1, 2, 4} with zero planes) over two views of the signed numerators
+// n in [-B, B], with colour_r(-n) = colour_r(n) + colour_r(-1):
+//   base view: index i = n, stored at bit u = i + 32*K0 + 31;
+//   odd view:  index i with n = 2i + 1 (odd numerators only), bit u = i + 32*K2;
+//              rows with an even denominator d only ever meet odd numerators
+//              (a primitive pair (b, d) with d even has b odd), so they read
+//              this half-size view (the reference's wheel rows for G = 2,
+//              src/census/engine32/vendor/research/baseline/baseline/previous/
+//              baseline/vendor/src/wheel_filter.hpp:14-46).
+// Planes of one profile are interleaved: word w of plane k sits at
+// [w * NPP + k], so one (vector) load fetches every plane of a word.
+// This replaces the reference's small_table / fine_labels / pack_pair kernels
+// (src/census/engine32/src/small_table.cuh:7-52).
 //
 // B200 design:
 //  * labels are computed only for primes q in the table (one Montgomery power
 //    each, kept in shared memory); every other n takes its label additively
 //    through a smallest-prime-factor chain n -> n / spf(n) (the colour is a
-//    character), so a table of ~10^6 entries costs ~8e4 powers, not 10^6;
-//  * each warp produces 32 consecutive labels per step and emits plane words
-//    with one ballot per plane bit: the negative half is one __brev'd ballot
-//    (aligned thanks to the +31 centring), the positive half is the previous
-//    step's ballot shifted by one with this step's first bit on top;
+//    character), so a table of ~10^6 entries costs ~6e4 powers, not 10^6;
+//  * each warp stages 32 consecutive labels per step in shared memory, then
+//    emits plane words profile by profile with one ballot per plane bit: the
+//    negative half of the base view is one __brev'd ballot (aligned by the
+//    +31 centring), the positive half is the previous step's ballot shifted
+//    by one with this step's first bit on top; two steps make one odd-view
+//    word per sign;
 //  * the same pass records the longest monochromatic stretch inside [1, B] per
 //    profile: a real run length, hence a certified lower bound on M (the role
 //    of the reference's seed_runs/finish_seed, small_table.cuh:64-136).
@@ -25,6 +36,8 @@
 namespace cz {
 
 constexpr int TABLE_THREADS = 1024;
+constexpr int TABLE_WARPS = TABLE_THREADS / 32;
+constexpr u32 TABLE_SUB = 8;       // steps staged per warp (even)
 
 struct TableArgs {
     const PrimeDesc *primes;
@@ -39,15 +52,24 @@ struct TableArgs {
     u32 chain_limit;
 };
 
-__device__ __forceinline__ u32 table_smem_bytes(u32 slots, u32 nq) {
-    return slots * 4u + slots * 2u + 8u + nq * 2u;
-}
+struct TabProf {            // per-profile constants of the CTA's prime
+    u32 r, magic, npp, sig;
+    u32 *base, *odd;
+};
+
+struct TabWarp {            // per-warp, per-profile carried state
+    u32 prevw[8][4];        // last base ballot per plane (positive carry)
+    u32 stp[8][4], stn[8][4];   // odd-view half words of the even step of a pair
+    u32 cc[8], clen[8], best[8];    // seed stretch: last colour, open length, best
+};
 
 __global__ void __launch_bounds__(TABLE_THREADS, 1)
 table_kernel(TableArgs a) {
     extern __shared__ u32 tsm[];
+    __shared__ TabProf tp[8];
+    __shared__ unsigned short lab[TABLE_WARPS][TABLE_SUB + 1][32];
+    __shared__ TabWarp tw[TABLE_WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nwarps = blockDim.x >> 5;
     for (u32 it = blockIdx.x; it < a.nsparse; it += gridDim.x) {
         const u32 pi = a.sparse_primes[it];
         const PrimeDesc P = a.primes[pi];
@@ -58,7 +80,7 @@ table_kernel(TableArgs a) {
         unsigned short *plab = reinterpret_cast<unsigned short *>(keys + slots + slots / 2u + 2u);
         build_root_hash(keys, hl, slots, M, P.z, P.m);
         const u32 KS = (P.B + 1u + 31u) / 32u + 1u;            // steps: n in [0, 32*KS)
-        const u32 nmax = 32u * KS;                               // exclusive
+        const u32 nmax = 32u * KS;
         u32 lo = 0, hi = a.n_small;                              // primes below nmax
         while (lo < hi) {
             u32 mid = (lo + hi) >> 1;
@@ -72,109 +94,154 @@ table_kernel(TableArgs a) {
             if (l == 0xFFFFu) { bad = 1; l = 0; }
             plab[i] = (unsigned short)l;
         }
-        __syncthreads();
         const u32 nprof = P.nprof;
-        const u32 mgm = magic_of(P.m);
-        u32 rr[8], mg[8], np[8], sg[8];
-        u32 *pl[8];
-#pragma unroll
-        for (int s = 0; s < 8; ++s) {
-            if (s < (int)nprof) {
-                const ProfDesc D = a.profs[P.first_prof + s];
-                rr[s] = D.r; np[s] = D.np; pl[s] = a.planes + D.plane_off;
-            } else {
-                rr[s] = 2; np[s] = 0; pl[s] = a.planes;
-            }
-            mg[s] = magic_of(rr[s]);
-            sg[s] = mod_small(P.sigma, rr[s], mg[s]);
+        if (threadIdx.x < nprof) {
+            const ProfDesc D = a.profs[P.first_prof + threadIdx.x];
+            TabProf t;
+            t.r = D.r;
+            t.magic = magic_of(D.r);
+            t.npp = D.npp;
+            t.sig = mod_small(P.sigma, D.r, t.magic);
+            t.base = a.planes + D.plane_off;
+            t.odd = a.planes + D.plane_off + (u64)P.nwords * D.npp;
+            tp[threadIdx.x] = t;
         }
-        const u32 K0 = P.K0, NW = P.nwords;
-        for (u32 w = threadIdx.x; w < NW; w += blockDim.x) {      // guard words
-            if (w + KS <= K0 || w >= K0 + KS) {
-#pragma unroll
-                for (int s = 0; s < 8; ++s) {
-                    if (s >= (int)nprof) break;
-                    for (u32 k = 0; k < np[s]; ++k) pl[s][(size_t)k * NW + w] = 0u;
-                }
-            }
+        {   // per-warp carried state
+            u32 *w = reinterpret_cast<u32 *>(&tw[warp]);
+            for (u32 i = lane; i < sizeof(TabWarp) / 4; i += 32) w[i] = 0u;
         }
-        const u32 per = (KS + nwarps - 1) / nwarps;
-        const u32 k0 = min(KS, warp * per), k1 = min(KS, k0 + per);
-        u32 prevw[8][4];
-        u32 carry_c[8], carry_len[8], seedbest[8];
-#pragma unroll
-        for (int s = 0; s < 8; ++s) {
-            carry_c[s] = 0xFFFFFFFFu; carry_len[s] = 0; seedbest[s] = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) prevw[s][k] = 0u;
+        __syncthreads();
+        if (lane < 8) tw[warp].cc[lane] = 0xFFFFFFFFu;
+        const u32 K0 = P.K0, NW = P.nwords, K2 = P.K2, NW2 = P.nwords2;
+        // guard words of both views (everything outside the written ranges)
+        for (u32 s = 0; s < nprof; ++s) {
+            const TabProf t = tp[s];
+            for (u32 w = threadIdx.x; w < NW; w += blockDim.x)
+                if (w + KS <= K0 || w >= K0 + KS)
+                    for (u32 k = 0; k < t.npp; ++k) t.base[(size_t)w * t.npp + k] = 0u;
+            const u32 half = (KS + 1u) / 2u;                     // step pairs
+            for (u32 w = threadIdx.x; w < NW2; w += blockDim.x)
+                if (w + half + 1u <= K2 || w >= K2 + half)
+                    for (u32 k = 0; k < t.npp; ++k) t.odd[(size_t)w * t.npp + k] = 0u;
         }
+        // warp chunk of steps [k0, k1), k0 even
+        u32 per = (KS + TABLE_WARPS - 1) / TABLE_WARPS;
+        per = (per + 1u) & ~1u;
+        const u32 k0 = min(KS, (u32)warp * per), k1 = min(KS, k0 + per);
         const u32 B = P.B;
-        for (u32 k = (k0 > 0 ? k0 - 1u : 0u); k < k1; ++k) {
-            const u32 n = 32u * k + (u32)lane;
-            u32 lab = 0;                       // label of n, additively along the spf chain
-            if (n >= 2 && n < a.chain_limit) {
-                u32 v = n;
-                for (int g = 0; g < 24 && v > 1u; ++g) {
-                    const uint2 c = a.chain[v];
-                    lab += plab[c.x];
-                    v = c.y;
+        __syncwarp();
+        for (u32 ks = k0; ks < k1; ks += TABLE_SUB) {
+            const u32 ke = min(k1, ks + TABLE_SUB);
+            const bool need_pre = (ks == k0 && k0 > 0);
+            // stage labels of steps [ks - need_pre, ke)
+            for (u32 k = ks - (need_pre ? 1u : 0u); k < ke; ++k) {
+                const u32 n = 32u * k + (u32)lane;
+                u32 l = 0;
+                if (n >= 2u && n < a.chain_limit) {
+                    u32 v = n;
+                    for (int g = 0; g < 24 && v > 1u; ++g) {
+                        const uint2 c = a.chain[v];
+                        l += plab[c.x];
+                        v = c.y;
+                    }
+                    if (v > 1u) bad = 1;
+                    l = mod_small(l, P.m, magic_of(P.m));
                 }
-                if (v > 1u) bad = 1;
-                lab = mod_small(lab, P.m, mgm);
+                lab[warp][k + 1u - ks][lane] = (unsigned short)l;   // slot 0 = pre-step
             }
-            const bool pre_step = (k0 > 0 && k == k0 - 1u);
-            const bool seedv = !pre_step && n >= 1u && n <= B;
-            const u32 V = __ballot_sync(0xFFFFFFFFu, seedv);
-            const u32 fv = V ? (u32)(__ffs(V) - 1) : 0u;
-            const u32 top = V ? 31u - __clz(V) : 0u;
+            __syncwarp();
+            for (u32 s = 0; s < nprof; ++s) {
+                const TabProf t = tp[s];
+                TabWarp &W = tw[warp];
+                u32 prevw[4], stp[4], stn[4];
 #pragma unroll
-            for (int s = 0; s < 8; ++s) {
-                if (s >= (int)nprof) break;
-                u32 c = mod_small(lab, rr[s], mg[s]);
-                u32 cn = c + sg[s];
-                if (cn >= rr[s]) cn -= rr[s];
-                if (n == 0) { c = 0; cn = 0; }
+                for (int b = 0; b < 4; ++b) { prevw[b] = W.prevw[s][b]; stp[b] = W.stp[s][b]; stn[b] = W.stn[s][b]; }
+                u32 cc = W.cc[s], clen = W.clen[s], best = W.best[s];
+                if (need_pre) {
+                    const u32 c = mod_small(lab[warp][0][lane], t.r, t.magic);
 #pragma unroll
-                for (int bit = 0; bit < 4; ++bit) {
-                    if (bit >= (int)np[s]) break;
-                    const u32 wp = __ballot_sync(0xFFFFFFFFu, (c >> bit) & 1u);
-                    const u32 wn = __ballot_sync(0xFFFFFFFFu, (cn >> bit) & 1u);
-                    if (!pre_step && lane == bit) {
-                        u32 *P0 = pl[s] + (size_t)bit * NW;
-                        P0[K0 - k] = __brev(wn);
-                        if (k >= 1) P0[K0 + k] = (prevw[s][bit] >> 1) | ((wp & 1u) << 31);
-                    }
-                    prevw[s][bit] = wp;
+                    for (int b = 0; b < 4; ++b)
+                        if (b < (int)t.npp) prevw[b] = __ballot_sync(0xFFFFFFFFu, (c >> b) & 1u);
                 }
-                if (!pre_step && V) {
+                for (u32 k = ks; k < ke; ++k) {
+                    const u32 n = 32u * k + (u32)lane;
+                    u32 c = mod_small(lab[warp][k + 1u - ks][lane], t.r, t.magic);
+                    u32 cn = c + t.sig;
+                    if (cn >= t.r) cn -= t.r;
+                    if (n == 0u) { c = 0u; cn = 0u; }
+                    const u32 co = __shfl_sync(0xFFFFFFFFu, c, 2 * (lane & 15) + 1);
+                    const u32 cno = __shfl_sync(0xFFFFFFFFu, cn, 2 * (lane & 15) + 1);
+                    const bool odd_step = (k & 1u) != 0u;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        if (b >= (int)t.npp) break;
+                        const u32 wp = __ballot_sync(0xFFFFFFFFu, (c >> b) & 1u);
+                        const u32 wn = __ballot_sync(0xFFFFFFFFu, (cn >> b) & 1u);
+                        const u32 hp = __ballot_sync(0xFFFFFFFFu, (co >> b) & 1u) & 0xFFFFu;
+                        const u32 hn = __ballot_sync(0xFFFFFFFFu, (cno >> b) & 1u) & 0xFFFFu;
+                        if (lane == b) {
+                            t.base[(size_t)(K0 - k) * t.npp + b] = __brev(wn);
+                            if (k >= 1u) t.base[(size_t)(K0 + k) * t.npp + b] = (prevw[b] >> 1) | ((wp & 1u) << 31);
+                            if (odd_step) {
+                                const u32 kap = k >> 1;
+                                t.odd[(size_t)(K2 + kap) * t.npp + b] = stp[b] | (hp << 16);
+                                t.odd[(size_t)(K2 - kap - 1u) * t.npp + b] = __brev(stn[b] | (hn << 16));
+                            }
+                        }
+                        prevw[b] = wp;
+                        if (!odd_step) { stp[b] = hp; stn[b] = hn; }
+                    }
+                    // odd-view word of a final unpaired even step
+                    if (!odd_step && k + 1u == KS) {
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            if (b >= (int)t.npp) break;
+                            if (lane == b) {
+                                const u32 kap = k >> 1;
+                                t.odd[(size_t)(K2 + kap) * t.npp + b] = stp[b];
+                                t.odd[(size_t)(K2 - kap - 1u) * t.npp + b] = __brev(stn[b]);
+                            }
+                        }
+                    }
                     // longest monochromatic stretch inside [1, B] (n = 1 starts a run)
-                    u32 pc = __shfl_up_sync(0xFFFFFFFFu, c, 1);
-                    if (lane == 0) pc = carry_c[s];
-                    const bool chg = seedv && (c != pc || n == 1u);
-                    const u32 C = __ballot_sync(0xFFFFFFFFu, chg);
-                    u32 clen = 0;
-                    if (chg) {
-                        const u32 below = C & ((1u << lane) - 1u);
-                        clen = below ? (u32)lane - (31u - __clz(below)) : carry_len[s] + (u32)lane - fv;
+                    const bool sv = n >= 1u && n <= B;
+                    const u32 V = __ballot_sync(0xFFFFFFFFu, sv);
+                    if (V) {
+                        const u32 fv = (u32)(__ffs(V) - 1), top = 31u - __clz(V);
+                        u32 pc = __shfl_up_sync(0xFFFFFFFFu, c, 1);
+                        if (lane == 0) pc = cc;
+                        const bool chg = sv && (c != pc || n == 1u);
+                        const u32 C = __ballot_sync(0xFFFFFFFFu, chg);
+                        u32 cl = 0;
+                        if (chg) {
+                            const u32 below = C & ((1u << lane) - 1u);
+                            cl = below ? (u32)lane - (31u - __clz(below)) : clen + (u32)lane - fv;
+                        }
+                        const u32 mx = __reduce_max_sync(0xFFFFFFFFu, cl);
+                        if (mx > best) best = mx;
+                        if (C) clen = top - (31u - __clz(C)) + 1u;
+                        else clen += top - fv + 1u;
+                        cc = __shfl_sync(0xFFFFFFFFu, c, top);
                     }
-                    const u32 mx = __reduce_max_sync(0xFFFFFFFFu, clen);
-                    if (mx > seedbest[s]) seedbest[s] = mx;
-                    if (C) carry_len[s] = top - (31u - __clz(C)) + 1u;
-                    else carry_len[s] += top - fv + 1u;
-                    carry_c[s] = __shfl_sync(0xFFFFFFFFu, c, top);
                 }
+                __syncwarp();
+                if (lane == 0) {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) { W.prevw[s][b] = prevw[b]; W.stp[s][b] = stp[b]; W.stn[s][b] = stn[b]; }
+                    W.cc[s] = cc; W.clen[s] = clen; W.best[s] = best;
+                }
+                __syncwarp();
             }
         }
         if (lane == 0) {
-#pragma unroll
-            for (int s = 0; s < 8; ++s) {
-                if (s >= (int)nprof) break;
-                u32 v = seedbest[s] > carry_len[s] ? seedbest[s] : carry_len[s];
+            for (u32 s = 0; s < nprof; ++s) {
+                const u32 v = max(tw[warp].best[s], tw[warp].clen[s]);
                 atomicMax(&a.state[P.first_prof + s].seed, v);
             }
         }
         bad = __syncthreads_or(bad);
         if (bad && threadIdx.x == 0) atomicOr(&a.state[P.first_prof].status, ST_LABEL);
+        __syncthreads();
     }
 }
 

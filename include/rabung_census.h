@@ -62,7 +62,8 @@ typedef struct cz_config {
     uint32_t screen;         /* 1: bilateral screen after the anchor filter */
     uint32_t sparse_blocks;  /* persistent filter grid (0: 2 per SM) */
     uint32_t use_graph;      /* 1: replay device work through a captured CUDA graph */
-    uint32_t reserved[6];
+    uint32_t cta_per_profile; /* CTAs sharing one profile's rows (L2 working set) */
+    uint32_t reserved[5];
 } cz_config;
 
 typedef struct cz_stats {

@@ -25,7 +25,7 @@ class cz_profile(ctypes.Structure):
 class cz_config(ctypes.Structure):
     _fields_ = [("device", i32), ("sparse_min_p", u32), ("cover_n", u32), ("q_cap", u32 * 10),
                 ("anchor_bits", u32), ("screen", u32), ("sparse_blocks", u32), ("use_graph", u32),
-                ("reserved", u32 * 6)]
+                ("cta_per_profile", u32), ("reserved", u32 * 5)]
 
 
 class cz_stats(ctypes.Structure):

@@ -30,6 +30,7 @@ class Tuning:
     screen: int = 1
     sparse_blocks: int = 0
     use_graph: int = 1
+    cta_per_profile: int = 2
 
 
 def _as_u32_array(values):
@@ -56,6 +57,7 @@ class Census:
         cfg.screen = t.screen
         cfg.sparse_blocks = t.sparse_blocks
         cfg.use_graph = t.use_graph
+        cfg.cta_per_profile = t.cta_per_profile
         h = ctypes.c_void_p()
         rc = self.lib.cz_open(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:

@@ -377,10 +377,11 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
         sa.prof_list = P<u32>(h->b_slist);
         sa.nlist = h->nsl;
         sa.next = P<u32>(h->b_counter);
+        sa.group = std::max(1u, h->cfg.cta_per_profile);
         sa.tune.anchor_bits = h->cfg.anchor_bits;
         sa.tune.screen = h->cfg.screen;
         u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : 2u * (u32)h->sms;
-        grid = std::min(grid, h->nsl);
+        grid = std::min(grid, h->nsl * sa.group);
         sparse_kernel<<<grid, SPARSE_WARPS * 32, 0, st>>>(sa);
         ++launches;
     }
@@ -470,6 +471,7 @@ int cz_default_config(cz_config *c) {
     c->screen = 1;
     c->sparse_blocks = 0;
     c->use_graph = 1;
+    c->cta_per_profile = 2;
     return CZ_OK;
 }
 

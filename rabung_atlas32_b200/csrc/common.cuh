@@ -148,7 +148,7 @@ struct ProfState {
     unsigned long long best;  // packed key of the best completed run
     u32 seed;                 // longest monochromatic stretch seen in [1, B]
     u32 firstnz;              // least n >= 1 with colour != 0 (prefix + 1)
-    u32 rows_done;
+    u32 rows_next;            // rows d handed out (sparse filter)
     u32 status;
     unsigned long long words;       // filter words visited
     unsigned long long completions; // exact completions run

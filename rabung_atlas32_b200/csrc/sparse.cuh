@@ -60,7 +60,8 @@ struct SparseArgs {
     const u32 *planes;
     const u32 *prof_list;     // global profile indices (sparse-routed)
     u32 nlist;
-    u32 *next;                // work counter (profiles handed out)
+    u32 *next;                // work counter: CTA slots handed out
+    u32 group;                // CTAs that share one profile (its rows)
     Tuning tune;
 };
 
@@ -323,15 +324,23 @@ __device__ __forceinline__ void filter_row(const ProfCtx &c, const View &vref, u
         }
         if (alive) {
             ++q.words;
-            u32 u = i0 + v.OFF;
+            const u32 u = i0 + v.OFF;
             u32 bw[NPP];
             Planes<NPP>::win(v.P, u, bw);
+            // stages in batches of SB: the batch's window loads are independent and
+            // issue back to back, so their latency is paid once per batch
+            constexpr int SB = NPP == 4 ? 2 : 4;
             u32 j = 1;
-            for (; j < t && alive; ++j) {
-                u -= dd;
-                alive &= ~mismatch<NPP>(v.P, u, bw);
+            while (j < t && alive) {
+                u32 m[SB];
+#pragma unroll
+                for (int k = 0; k < SB; ++k)
+                    m[k] = (j + (u32)k < t) ? mismatch<NPP>(v.P, u - (j + (u32)k) * dd, bw) : 0u;
+#pragma unroll
+                for (int k = 0; k < SB; ++k) alive &= ~m[k];
+                j += SB;
             }
-            q.tests += j * (u32)NPP;
+            q.tests += min(j, t) * (u32)NPP;
         }
         const bool has = alive != 0u;
         const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
@@ -350,15 +359,15 @@ __device__ __forceinline__ void filter_row(const ProfCtx &c, const View &vref, u
 
 __global__ void __launch_bounds__(SPARSE_WARPS * 32, 2)
 sparse_kernel(SparseArgs a) {
-    __shared__ u32 s_item, s_row, s_err;
+    __shared__ u32 s_item, s_err;
     __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];      // candidates awaiting completion
     __shared__ uint2 sbuf[SPARSE_WARPS][CAND_CAP];     // (index, alive) words awaiting the screen
     __shared__ ProfCtx s_ctx;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (;;) {
         if (threadIdx.x == 0) {
-            s_item = atomicAdd(a.next, 1u);
-            s_row = 1u;
+            // a.group consecutive CTA slots share one profile
+            s_item = atomicAdd(a.next, 1u) / a.group;
             s_err = 0u;
             if (s_item < a.nlist) {
                 const u32 gprof = a.prof_list[s_item];
@@ -389,7 +398,7 @@ sparse_kernel(SparseArgs a) {
         Cand *cb = cbuf[warp];
         for (;;) {
             u32 d = 0;
-            if (lane == 0) d = atomicAdd(&s_row, 1u);
+            if (lane == 0) d = atomicAdd(&st->rows_next, 1u) + 1u;     // rows in increasing d
             d = __shfl_sync(0xFFFFFFFFu, d, 0);
             if (d > c.D) break;
             // row parameters from the verified maximum so far (<= M)

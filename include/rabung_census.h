@@ -41,6 +41,7 @@ extern "C" {
 #define CZ_EINVAL 1   /* bad argument (not prime, out of domain, buffer too small) */
 #define CZ_ECUDA 2    /* CUDA error */
 #define CZ_EREFUSED 3 /* a device status check failed: the whole request is refused */
+#define CZ_ELIMIT 4   /* request exceeds the fixed limits of cz_census_dense_noalloc */
 
 /* One (p, r) profile, 32 bytes.  Records come grouped by prime in input
  * order and, within a prime, by ascending r. */
@@ -110,6 +111,21 @@ int cz_a4(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t *a4_out);
  * one three-input logic op on 32-bit words), kind 1 = 32-bit Montgomery
  * products per second. */
 int cz_microbench(cz_handle *h, uint32_t kind, double *per_second);
+
+/* Dense census that allocates no memory (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc -- code running inside a CUDA graph
+ * capture into a pool it does not own, plugins in a host process that owns the
+ * device memory budget, allocator-free services.  All device scratch is one
+ * fixed 2 MiB array inside the library, held by every GPU that loads the
+ * library until the process exits.  Limits: n <= 64 primes, each p < 4,194,304
+ * (CZ_ELIMIT beyond them).  primes and out are host arrays as in cz_census
+ * (out holds cz_count_profiles() records); stream is a cudaStream_t (NULL for
+ * the legacy default stream) on the current device; the call returns after
+ * that stream has finished.  The first call on a device resolves the array's
+ * device address and should come before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race. */
+int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_profile *out, uint32_t out_cap,
+                            void *stream);
 
 /* Reference-compatible adapter (src/census/engine32/src/baseline_bridge.cu:7,21-27):
  * profile of one prime for the orders in `mask` (bit r-2), M into out[r] and

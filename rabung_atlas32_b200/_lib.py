@@ -12,7 +12,7 @@ from pathlib import Path
 from .build import LIB
 
 CZ_DENSE, CZ_SPARSE, CZ_AUTO, CZ_A4, CZ_VERIFY = 1, 2, 3, 4, 8
-CZ_OK, CZ_EINVAL, CZ_ECUDA, CZ_EREFUSED = 0, 1, 2, 3
+CZ_OK, CZ_EINVAL, CZ_ECUDA, CZ_EREFUSED, CZ_ELIMIT = 0, 1, 2, 3, 4
 
 u32, u64, i32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
 
@@ -41,7 +41,8 @@ class cz_stats(ctypes.Structure):
 
 
 EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_count_profiles",
-           "cz_census", "cz_replay", "cz_a4", "cz_microbench", "baseline_init", "baseline_profile"]
+           "cz_census", "cz_replay", "cz_a4", "cz_microbench", "cz_census_dense_noalloc", "baseline_init",
+           "baseline_profile"]
 
 _lib = None
 
@@ -75,6 +76,9 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.cz_a4.restype = ctypes.c_int
     L.cz_microbench.argtypes = [H, u32, ctypes.POINTER(ctypes.c_double)]
     L.cz_microbench.restype = ctypes.c_int
+    L.cz_census_dense_noalloc.argtypes = [ctypes.POINTER(u32), u32, ctypes.POINTER(cz_profile), u32,
+                                          ctypes.c_void_p]
+    L.cz_census_dense_noalloc.restype = ctypes.c_int
     L.baseline_init.argtypes = [ctypes.c_uint]
     L.baseline_init.restype = None
     L.baseline_profile.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),

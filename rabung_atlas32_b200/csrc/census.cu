@@ -700,6 +700,175 @@ int cz_microbench(cz_handle *h, uint32_t kind, double *per_second) {
     return CZ_OK;
 }
 
+// ---- dense census without device allocation ---------------------------------
+//
+// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
+// being captured into a pool it does not own, plugins inside a host process
+// that owns the device's memory budget, or allocator-free embedded services.
+// cz_census_dense_noalloc serves them.  Its only device scratch is the
+// file-scope array below (NOALLOC_BYTES, held by every GPU that loads this
+// library until the process exits); descriptors, run summaries, per-profile
+// state and output records are carved out of it.  The host side uses fixed
+// stack arrays only.  Calls share the array: two calls that overlap on the GPU
+// (different streams, or different host threads) race.
+
+constexpr u32 NOALLOC_BYTES = 2u << 20;          // 2 MiB
+constexpr u32 NOALLOC_MAX_PRIMES = 64;
+constexpr u32 NOALLOC_MAX_P = 1u << 22;          // p < 4,194,304
+constexpr u32 NOALLOC_MAX_PROFILES = NOALLOC_MAX_PRIMES * 8u;
+// chunks per profile for p < 2^22: ceil(ceil(2^21 / DENSE_SEG) / DENSE_WARPS)
+constexpr u32 NOALLOC_MAX_CHUNKS = ((1u << 21) / DENSE_SEG + DENSE_WARPS - 1u) / DENSE_WARPS;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+
+struct NoallocLayout {      // byte offsets inside the scratch array (256-aligned)
+    size_t primes, profs, state, chunk, summp, didx, dlist, dpre, out, summ, end;
+};
+
+constexpr size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+constexpr NoallocLayout noalloc_layout() {
+    NoallocLayout L{};
+    size_t o = 0;
+    L.primes = o; o = al256(o + sizeof(PrimeDesc) * NOALLOC_MAX_PRIMES);
+    L.profs = o;  o = al256(o + sizeof(ProfDesc) * NOALLOC_MAX_PROFILES);
+    L.state = o;  o = al256(o + sizeof(ProfState) * NOALLOC_MAX_PROFILES);
+    L.chunk = o;  o = al256(o + 4 * (NOALLOC_MAX_PRIMES + 1));
+    L.summp = o;  o = al256(o + 4 * NOALLOC_MAX_PRIMES);
+    L.didx = o;   o = al256(o + 4 * NOALLOC_MAX_PRIMES);
+    L.dlist = o;  o = al256(o + 4 * NOALLOC_MAX_PROFILES);
+    L.dpre = o;   o = al256(o + 4 * NOALLOC_MAX_PROFILES);
+    L.out = o;    o = al256(o + sizeof(OutRecord) * NOALLOC_MAX_PROFILES);
+    L.summ = o;   o = al256(o + sizeof(Summ) * NOALLOC_MAX_PROFILES * NOALLOC_MAX_CHUNKS);
+    L.end = o;
+    return L;
+}
+static_assert(noalloc_layout().end <= NOALLOC_BYTES, "static scratch too small for its limits");
+
+// device address of the scratch array, resolved once per device with that
+// device current (the host-side name is only a stand-in for the symbol)
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_ptr[64] = {};
+
+int noalloc_setup(int dev, unsigned char **out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (dev < 0 || dev >= 64) return CZ_EINVAL;
+    if (!g_noalloc_ptr[dev]) {
+        void *ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return CZ_ECUDA;
+        if (cudaFuncSetAttribute(dense_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) !=
+            cudaSuccess)
+            return CZ_ECUDA;
+        g_noalloc_ptr[dev] = static_cast<unsigned char *>(ptr);
+    }
+    *out = g_noalloc_ptr[dev];
+    return CZ_OK;
+}
+
+}  // namespace
+
+extern "C" int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_profile *out, uint32_t out_cap,
+                                       void *stream) {
+    if (n == 0) return CZ_OK;
+    if (!primes || !out) return CZ_EINVAL;
+    if (n > NOALLOC_MAX_PRIMES) return CZ_ELIMIT;
+    // host plan on fixed arrays (the dense route of plan())
+    PrimeDesc hp[NOALLOC_MAX_PRIMES];
+    ProfDesc hprof[NOALLOC_MAX_PROFILES];
+    u32 chunk[NOALLOC_MAX_PRIMES + 1], summp[NOALLOC_MAX_PRIMES], didx[NOALLOC_MAX_PRIMES];
+    u32 dlist[NOALLOC_MAX_PROFILES];
+    u32 nprof = 0, nd = 0, summ_slots = 0;
+    chunk[0] = 0;
+    for (u32 i = 0; i < n; ++i) {
+        const u32 p = primes[i];
+        if (p < 2u) return CZ_EINVAL;
+        if (p >= NOALLOC_MAX_P) return CZ_ELIMIT;
+        PrimeDesc P{};
+        P.p = p;
+        P.mask = p > 2u ? mask_of(p) : 0u;
+        P.m = lcm_of_mask(P.mask);
+        P.e = P.mask ? (p - 1u) / P.m : 0u;
+        P.first_prof = nprof;
+        P.nprof = popc(P.mask);
+        P.route = P.nprof ? 1u : 0u;
+        if (P.nprof) {
+            const u32 nh = (p - 1u) / 2u;
+            const u32 nseg = (nh + DENSE_SEG - 1u) / DENSE_SEG;
+            const u32 nch = (nseg + DENSE_WARPS - 1u) / DENSE_WARPS;
+            didx[nd] = i;
+            summp[nd] = summ_slots;
+            summ_slots += nch * P.nprof;
+            chunk[nd + 1] = chunk[nd] + nch;
+            for (u32 r = 2; r <= 9; ++r) {
+                if (!(P.mask & (1u << (r - 2)))) continue;
+                ProfDesc D{};
+                D.prime = i; D.r = r; D.np = planes_for(r); D.npp = planes_stored(r);
+                D.out_slot = nprof; D.local = nd;
+                dlist[nprof] = nprof;
+                hprof[nprof++] = D;
+            }
+            ++nd;
+        }
+        hp[i] = P;
+    }
+    if (out_cap < nprof) return CZ_EINVAL;
+    if (nprof == 0) return CZ_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CZ_ECUDA;
+    unsigned char *base = nullptr;
+    int rc = noalloc_setup(dev, &base);
+    if (rc) return rc;
+    constexpr NoallocLayout L = noalloc_layout();
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    auto h2d = [&](size_t off, const void *src, size_t bytes) {
+        return cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    };
+    if (!h2d(L.primes, hp, sizeof(PrimeDesc) * n) || !h2d(L.profs, hprof, sizeof(ProfDesc) * nprof) ||
+        !h2d(L.chunk, chunk, 4ull * (nd + 1)) || !h2d(L.summp, summp, 4ull * nd) || !h2d(L.didx, didx, 4ull * nd) ||
+        !h2d(L.dlist, dlist, 4ull * nprof))
+        return CZ_ECUDA;
+    PrimeDesc *dP = reinterpret_cast<PrimeDesc *>(base + L.primes);
+    ProfDesc *dD = reinterpret_cast<ProfDesc *>(base + L.profs);
+    ProfState *dS = reinterpret_cast<ProfState *>(base + L.state);
+    // setup_kernel re-initialises every ProfState this call uses
+    setup_kernel<<<(n + 127) / 128, 128, 0, st>>>(dP, dD, dS, n);
+    u32 max_slots = 8;
+    for (u32 i = 0; i < n; ++i) max_slots = std::max(max_slots, hash_slots(hp[i].m));
+    DenseArgs da;
+    da.primes = dP;
+    da.dense_idx = reinterpret_cast<u32 *>(base + L.didx);
+    da.profs = dD;
+    da.chunk_prefix = reinterpret_cast<u32 *>(base + L.chunk);
+    da.summ_prefix = reinterpret_cast<u32 *>(base + L.summp);
+    da.nprimes = nd;
+    da.nchunks = chunk[nd];
+    da.summ = reinterpret_cast<Summ *>(base + L.summ);
+    da.state = dS;
+    dense_scan_kernel<<<std::max(1u, std::min(chunk[nd], 1184u)), DENSE_WARPS * 32, max_slots * 6u + 16u, st>>>(da);
+    DenseMergeArgs ma;
+    ma.primes = dP;
+    ma.profs = dD;
+    ma.chunk_prefix = da.chunk_prefix;
+    ma.summ_prefix = da.summ_prefix;
+    ma.nprimes = nd;
+    ma.summ = da.summ;
+    ma.state = dS;
+    ma.prefix_out = reinterpret_cast<u32 *>(base + L.dpre);
+    dense_merge_kernel<<<(nprof + 7) / 8, 256, 0, st>>>(ma, reinterpret_cast<u32 *>(base + L.dlist), nprof);
+    OutRecord *dO = reinterpret_cast<OutRecord *>(base + L.out);
+    finalize_kernel<<<(nprof + 127) / 128, 128, 0, st>>>(dP, dD, dS, ma.prefix_out, nprof, 0u, dO);
+    if (cudaGetLastError() != cudaSuccess) return CZ_ECUDA;
+    static_assert(sizeof(OutRecord) == sizeof(cz_profile), "record layout");
+    if (cudaMemcpyAsync(out, dO, sizeof(OutRecord) * nprof, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return CZ_ECUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return CZ_ECUDA;
+    for (u32 g = 0; g < nprof; ++g)
+        if (out[g].status) return CZ_EREFUSED;
+    return CZ_OK;
+}
+
 // ---- reference-compatible adapter -------------------------------------------
 static cz_handle *g_base = nullptr;
 

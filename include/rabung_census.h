@@ -64,13 +64,18 @@ typedef struct cz_config {
     uint32_t sparse_blocks;  /* persistent filter grid (0: 2 per SM) */
     uint32_t use_graph;      /* 1: replay device work through a captured CUDA graph */
     uint32_t cta_per_profile; /* CTAs sharing one profile's rows (L2 working set) */
-    uint32_t reserved[5];
+    uint32_t l1_carveout;    /* filter's preferred shared-memory carveout, % (>100: driver default) */
+    uint32_t speculate;      /* 1: speculative thresholds floor(log_r p - margin), re-run on a miss */
+    uint32_t spec_margin10[10];  /* margin per order r, in tenths */
+    uint32_t reserved[3];
 } cz_config;
 
 typedef struct cz_stats {
     float ms_setup, ms_table, ms_sparse, ms_dense, ms_a4, ms_finalize, ms_device;
     float ms_h2d, ms_d2h;
     uint32_t n_primes, n_dense, n_sparse, n_profiles, n_fallback;
+    uint32_t n_respec;              /* primes re-run because a speculative threshold missed */
+    float ms_respec;                /* device time of that re-run */
     uint32_t kernels;               /* kernel launches of the call */
     uint64_t words, completions;    /* sparse filter words visited, exact completions */
     uint64_t tests;                 /* plane-window comparisons executed by the filter */

@@ -25,7 +25,8 @@ class cz_profile(ctypes.Structure):
 class cz_config(ctypes.Structure):
     _fields_ = [("device", i32), ("sparse_min_p", u32), ("cover_n", u32), ("q_cap", u32 * 10),
                 ("anchor_bits", u32), ("screen", u32), ("sparse_blocks", u32), ("use_graph", u32),
-                ("cta_per_profile", u32), ("reserved", u32 * 5)]
+                ("cta_per_profile", u32), ("l1_carveout", u32), ("speculate", u32),
+                ("spec_margin10", u32 * 10), ("reserved", u32 * 3)]
 
 
 class cz_stats(ctypes.Structure):
@@ -33,7 +34,8 @@ class cz_stats(ctypes.Structure):
                 ("ms_dense", ctypes.c_float), ("ms_a4", ctypes.c_float), ("ms_finalize", ctypes.c_float),
                 ("ms_device", ctypes.c_float), ("ms_h2d", ctypes.c_float), ("ms_d2h", ctypes.c_float),
                 ("n_primes", u32), ("n_dense", u32), ("n_sparse", u32), ("n_profiles", u32),
-                ("n_fallback", u32), ("kernels", u32), ("words", u64), ("completions", u64),
+                ("n_fallback", u32), ("n_respec", u32), ("ms_respec", ctypes.c_float),
+                ("kernels", u32), ("words", u64), ("completions", u64),
                 ("tests", u64), ("h2d_bytes", u64), ("d2h_bytes", u64)]
 
     def as_dict(self) -> dict:

@@ -31,6 +31,9 @@ class Tuning:
     sparse_blocks: int = 0
     use_graph: int = 1
     cta_per_profile: int = 2
+    l1_carveout: int = 20
+    speculate: int = 1
+    spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 15, 15, 15, 15)
 
 
 def _as_u32_array(values):
@@ -58,6 +61,10 @@ class Census:
         cfg.sparse_blocks = t.sparse_blocks
         cfg.use_graph = t.use_graph
         cfg.cta_per_profile = t.cta_per_profile
+        cfg.l1_carveout = t.l1_carveout
+        cfg.speculate = t.speculate
+        for r in range(10):
+            cfg.spec_margin10[r] = t.spec_margin10[r]
         h = ctypes.c_void_p()
         rc = self.lib.cz_open(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:

@@ -162,7 +162,19 @@ bool build_static_tables(cz_handle *h) {
 
 u32 q_for(const cz_config &c, u32 r) { return c.q_cap[r] ? c.q_cap[r] : 16u; }
 
+// speculative threshold: floor(log_r p - margin_r), a low quantile of M for
+// random-looking colourings (M ~ log_r p); 0 disables
+u32 qspec_for(const cz_config &c, u32 p, u32 r, bool allow) {
+    if (!allow || !c.speculate) return 0u;
+    const double lg = std::log((double)p) / std::log((double)r);
+    const double m = c.spec_margin10[r] / 10.0;
+    const double v = std::floor(lg - m);
+    return v < 3.0 ? 0u : (u32)v;
+}
+
 // host plan of one call
+constexpr u32 CZ_NOSPEC = 1u << 16;      // internal: plan without speculative thresholds
+
 int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
     const cz_config &c = h->cfg;
     h->hp.assign(n, PrimeDesc{});
@@ -238,6 +250,7 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
             if (sparse) {
                 D.Q = q_for(c, r);
                 D.D = Ds[k];
+                D.qspec = qspec_for(c, p, r, !(flags & CZ_NOSPEC));
                 D.plane_off = plane_words;              // multiple of 4 words: vector loads align
                 plane_words += ((u64)D.npp * (P.nwords + P.nwords2) + 3ull) & ~3ull;
                 D.local = (u32)h->h_sidx.size() - 1u;
@@ -436,11 +449,16 @@ void read_times(cz_handle *h, cz_stats *s) {
     cudaEventElapsedTime(&s->ms_device, h->ev[0], h->ev[6]);
 }
 
-int check_records(cz_handle *h, std::vector<u32> *fallback) {
+int check_records(cz_handle *h, std::vector<u32> *fallback, std::vector<u32> *respec = nullptr) {
     for (u32 g = 0; g < h->nprof; ++g) {
         const OutRecord &o = h->hout[g];
         if (o.status) {
             const PrimeDesc &P = h->hp[h->hprof[g].prime];
+            if (respec && P.route == 2u && o.status == ST_SPEC) {
+                if (respec->empty() || respec->back() != h->hprof[g].prime)
+                    respec->push_back(h->hprof[g].prime);
+                continue;
+            }
             if (fallback && P.route == 2u && !(o.status & (ST_ROOT | ST_LABEL | ST_VERIFY))) {
                 if (fallback->empty() || fallback->back() != h->hprof[g].prime)
                     fallback->push_back(h->hprof[g].prime);
@@ -472,6 +490,10 @@ int cz_default_config(cz_config *c) {
     c->sparse_blocks = 0;
     c->use_graph = 1;
     c->cta_per_profile = 2;
+    c->l1_carveout = 20;
+    c->speculate = 1;
+    const u32 sm[10] = {0, 0, 30, 20, 15, 15, 15, 15, 15, 15};
+    for (int r = 0; r < 10; ++r) c->spec_margin10[r] = sm[r];
     return CZ_OK;
 }
 
@@ -494,6 +516,10 @@ int cz_open(const cz_config *cfg, cz_handle **out) {
     for (auto &e : h->ev) cudaEventCreate(&e);
     cudaFuncSetAttribute(table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_DYN_SMEM);
     cudaFuncSetAttribute(dense_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    // the filter needs ~20 KB of shared memory per CTA: give the rest of the
+    // unified L1/shared array to L1, where the colour planes are cached
+    if (h->cfg.l1_carveout <= 100)
+        cudaFuncSetAttribute(sparse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)h->cfg.l1_carveout);
     if (!build_static_tables(h)) { cz_close(h); return CZ_ECUDA; }
     *out = h;
     return CZ_OK;
@@ -574,24 +600,44 @@ static int census_impl(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_
         cudaMemcpy(&a4err, P<u32>(h->b_counter) + 8, 4, cudaMemcpyDeviceToHost);
         if (a4err) { h->err = "refused: A4 point count not certified"; return CZ_EREFUSED; }
     }
-    std::vector<u32> fb;
-    rc = check_records(h, allow_fallback ? &fb : nullptr);
+    std::vector<u32> fb, rs;
+    rc = check_records(h, allow_fallback ? &fb : nullptr, allow_fallback ? &rs : nullptr);
     if (rc) return rc;
     for (u32 g = 0; g < h->nprof; ++g) {
         const OutRecord &o = h->hout[g];
         cz_profile &d = out[g];
         d.p = o.p; d.r = o.r; d.M = o.M; d.L = o.L; d.witness = o.witness; d.status = o.status; d.K = o.K;
     }
+    // the re-runs below re-plan the handle: take the primes and record slots first
+    std::vector<u32> fb_p, fb_first;
+    for (u32 pi : fb) { fb_p.push_back(h->hp[pi].p); fb_first.push_back(h->hp[pi].first_prof); }
+    if (!rs.empty()) {
+        // profiles whose best run stayed below the speculative threshold: the
+        // speculation was not certified, re-run those primes without it
+        std::vector<u32> sub;
+        for (u32 pi : rs) sub.push_back(h->hp[pi].p);
+        std::vector<u32> first(rs.size());
+        for (size_t k = 0; k < rs.size(); ++k) first[k] = h->hp[rs[k]].first_prof;
+        const u32 fflags = (flags & ~CZ_A4) | CZ_NOSPEC;
+        std::vector<cz_profile> tmp(cz_count_profiles(sub.data(), (u32)sub.size()));
+        cz_stats s2{};
+        rc = census_impl(h, sub.data(), (u32)sub.size(), fflags, tmp.data(), (u32)tmp.size(), nullptr, &s2, true);
+        if (rc) return rc;
+        u32 t = 0;
+        for (size_t k = 0; k < rs.size(); ++k) {
+            const u32 np = popc(mask_of(sub[k]));
+            for (u32 j = 0; j < np; ++j) out[first[k] + j] = tmp[t++];
+        }
+        s.n_respec = (u32)rs.size();
+        s.ms_respec = s2.ms_device;
+        h->have_plan = false;
+    }
     if (!fb.empty()) {
         // sparse primes whose seed could not certify a threshold: dense re-run
-        std::vector<u32> sub, slot;
-        for (u32 pi : fb) sub.push_back(h->hp[pi].p);
-        std::vector<u32> first(fb.size());
-        for (size_t k = 0; k < fb.size(); ++k) first[k] = h->hp[fb[k]].first_prof;
+        const std::vector<u32> &sub = fb_p, &first = fb_first;
         const u32 fflags = (flags & ~CZ_AUTO & ~CZ_A4) | CZ_DENSE;
         std::vector<cz_profile> tmp(cz_count_profiles(sub.data(), (u32)sub.size()));
         cz_stats s2{};
-        std::vector<OutRecord> keep_out = h->hout;
         rc = census_impl(h, sub.data(), (u32)sub.size(), fflags, tmp.data(), (u32)tmp.size(), nullptr, &s2, false);
         if (rc) return rc;
         u32 t = 0;

@@ -141,6 +141,7 @@ struct ProfDesc {
     u64 plane_off;   // word offset of plane 0 in the plane pool
     u32 omega[9];    // Montgomery omega^j, omega = z^(m/r), j < r
     u32 local;       // index of the prime within its route's list
+    u32 qspec;       // speculative threshold (0: none); exact if the best run reaches it
 };
 
 // device-written per-profile results
@@ -165,6 +166,7 @@ enum : u32 {
     ST_A4 = 1u << 5,         // point count not certified
     ST_QUEUE = 1u << 6,      // candidate buffer overflow
     ST_COVER = 1u << 7,      // cover certificate out of domain
+    ST_SPEC = 1u << 8,       // best run below the speculative threshold: re-run without it
 };
 
 }  // namespace cz

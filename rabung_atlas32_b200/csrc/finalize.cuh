@@ -97,7 +97,8 @@ __global__ void finalize_kernel(const PrimeDesc *primes, const ProfDesc *profs, 
     const u32 p = P.p, r = D.r, ex = (p - 1u) / r;
     u32 status = P.status | S.status;
     const u32 Mlen = key_len(S.best), w = key_witness(S.best);
-    if (S.best == 0ull) status |= ST_VERIFY;
+    if (S.best == 0ull && !(D.qspec && P.route == 2u)) status |= ST_VERIFY;
+    if (P.route == 2u && D.qspec && Mlen < D.qspec) status |= ST_SPEC;
     u32 L;
     if (P.route == 1u) {
         L = dense_prefix[g];

@@ -359,7 +359,7 @@ __device__ __forceinline__ void filter_row(const ProfCtx &c, const View &vref, u
 
 __global__ void __launch_bounds__(SPARSE_WARPS * 32, 2)
 sparse_kernel(SparseArgs a) {
-    __shared__ u32 s_item, s_err;
+    __shared__ u32 s_item, s_err, s_qspec;
     __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];      // candidates awaiting completion
     __shared__ uint2 sbuf[SPARSE_WARPS][CAND_CAP];     // (index, alive) words awaiting the screen
     __shared__ ProfCtx s_ctx;
@@ -384,6 +384,7 @@ sparse_kernel(SparseArgs a) {
                              (i32)((PR.B - 1u) / 2u), 2u, 1u};
                 for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
                 s_ctx = c;
+                s_qspec = PD.qspec;
             }
         }
         __syncthreads();
@@ -392,6 +393,7 @@ sparse_kernel(SparseArgs a) {
         const ProfCtx &c = s_ctx;
         ProfState *st = a.state + a.prof_list[item];
         const u32 seed = *(volatile u32 *)&st->seed;
+        const u32 qspec = s_qspec;
         const u32 tpref = anchor_pref(c.r, a.tune.anchor_bits);
         WarpQ q{0, 0, 0, 0, 0, 0, 0};
         uint2 *sb = sbuf[warp];
@@ -403,7 +405,10 @@ sparse_kernel(SparseArgs a) {
             if (d > c.D) break;
             // row parameters from the verified maximum so far (<= M)
             const u64 bk = *(volatile unsigned long long *)&st->best;
-            const u32 blen = key_len(bk) > seed ? key_len(bk) : seed;
+            u32 blen = key_len(bk) > seed ? key_len(bk) : seed;
+            // a speculative threshold: every run >= blen is still completed; if the
+            // final best stays below qspec the profile is re-run without it
+            if (qspec > blen) blen = qspec;
             const u32 q_ = blen < c.Q ? blen : c.Q;
             if (q_ < 3u) { q.err |= 2u; break; }
             const u32 t = tpref < q_ ? (tpref < 2u ? 2u : tpref) : q_;

@@ -158,3 +158,16 @@ def test_replay_bit_identical(eng):
     assert st["n_profiles"] == sum(len(r.profiles) for r in a)
     b = eng.profiles(ps, mode="sparse", a4=False)
     assert tup(a) == tup(b)
+
+
+def test_speculation_miss_rerun_exact():
+    """Speculative thresholds at floor(log_r p) (margin 0) miss often; every miss
+    is re-run without speculation and the records equal the unspeculated ones."""
+    from rabung_atlas32_b200.census import Census, Tuning
+    ps = sieve.primes_ending(4294967291, 96)
+    with Census(tuning=Tuning(speculate=0)) as c0:
+        want = tup(c0.profiles(ps, mode="sparse", a4=False))
+    with Census(tuning=Tuning(speculate=1, spec_margin10=(0,) * 10)) as c1:
+        got = tup(c1.profiles(ps, mode="sparse", a4=False))
+        assert c1.last_stats["n_respec"] > 0
+    assert got == want

@@ -48,6 +48,52 @@ TOP = 4294967291
 BLOCK = 4096
 
 
+def uneven_blocks(rank: int = 0, nblocks: int = 64, size: int = BLOCK, seed: int = 20261203) -> list:
+    """64 blocks of 4096 consecutive primes, starts log-uniform over [2^16, 2^32)
+    from a fixed seed (rank k draws from seed + k)."""
+    import numpy as np
+    from rabung_atlas32_b200 import sieve
+    rng = np.random.default_rng(seed + rank)
+    starts = sorted(int(x) for x in np.exp2(rng.uniform(16, 32, nblocks)))
+    return [sieve.primes_from(s, size) for s in starts]
+
+
+def uneven_arm(args) -> None:
+    """Batched uneven census: all blocks in one call (persistent kernels, waves
+    when the plane pool exceeds its budget) vs one block per call."""
+    from rabung_atlas32_b200.census import Census
+    blocks = uneven_blocks(int(os.environ.get("RANK", "0")))
+    flat = [p for b in blocks for p in b]
+    eng = Census()
+    nprof = eng.count_profiles(flat)
+    for _ in range(max(1, args.warmup - 2)):
+        eng.raw(flat, mode="auto", a4=True)
+    dev, e2e, waves = [], [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out, a4, st = eng.raw(flat, mode="auto", a4=True)
+        e2e.append(time.perf_counter() - t0)
+        dev.append(st["ms_device"] / 1000.0)
+        waves = st["waves"]
+    batched = [(o.p, o.r, o.M, o.L, o.witness) for o in out[:nprof]] + [tuple(a4)]
+    plain_dev, plain_e2e, plain_rec, plain_a4 = 0.0, 0.0, [], []
+    for b in blocks:
+        t0 = time.perf_counter()
+        o, a, st = eng.raw(b, mode="auto", a4=True)
+        plain_e2e += time.perf_counter() - t0
+        plain_dev += st["ms_device"] / 1000.0
+        plain_rec += [(x.p, x.r, x.M, x.L, x.witness) for x in o[:eng.count_profiles(b)]]
+        plain_a4 += a
+    same = batched == plain_rec + [tuple(plain_a4)]
+    print(json.dumps({
+        "metric": "profiles/s, batched uneven census (64 blocks x 4096 primes, log-uniform starts in [2^16, 2^32))",
+        "value": round(nprof / (sum(dev) / len(dev)), 1), "unit": "profiles/s", "steps": args.steps,
+        "primes": len(flat), "profiles": nprof, "waves": waves,
+        "e2e": round(nprof / (sum(e2e) / len(e2e)), 1),
+        "plain_one_block_per_call": {"value": round(nprof / plain_dev, 1), "e2e": round(nprof / plain_e2e, 1)},
+        "batched_over_plain": round(plain_dev / (sum(dev) / len(dev)), 3), "bit_identical": same}))
+
+
 def workload(rank: int) -> list:
     from rabung_atlas32_b200 import sieve
     hi = TOP
@@ -183,11 +229,21 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="top", choices=["top", "uneven", "serve"])
+    ap.add_argument("--requests", type=int, default=10000)
+    ap.add_argument("--rate", type=float, default=40.0, help="offered load, requests/s (serve)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.workload == "uneven":
+        uneven_arm(args)
+        return
+    if args.workload == "serve":
+        from rabung_atlas32_b200 import serving
+        print(json.dumps(serving.benchmark(requests=args.requests, rate=args.rate, seed=20261203)))
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -67,7 +67,8 @@ typedef struct cz_config {
     uint32_t l1_carveout;    /* filter's preferred shared-memory carveout, % (>100: driver default) */
     uint32_t speculate;      /* 1: speculative thresholds floor(log_r p - margin), re-run on a miss */
     uint32_t spec_margin10[10];  /* margin per order r, in tenths */
-    uint32_t reserved[3];
+    uint32_t plane_budget_mb;    /* plane pool per wave; larger batches run as consecutive waves */
+    uint32_t reserved[2];
 } cz_config;
 
 typedef struct cz_stats {
@@ -76,6 +77,7 @@ typedef struct cz_stats {
     uint32_t n_primes, n_dense, n_sparse, n_profiles, n_fallback;
     uint32_t n_respec;              /* primes re-run because a speculative threshold missed */
     float ms_respec;                /* device time of that re-run */
+    uint32_t waves;                 /* consecutive waves the batch ran as */
     uint32_t kernels;               /* kernel launches of the call */
     uint64_t words, completions;    /* sparse filter words visited, exact completions */
     uint64_t tests;                 /* plane-window comparisons executed by the filter */
@@ -106,6 +108,20 @@ int cz_census(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags,
  * to time the device path alone.  Results land in the same device buffers and
  * are checked; stats receives the device times. */
 int cz_replay(cz_handle *h, cz_stats *stats);
+
+/* Device memory the colour planes of these primes would take (admission
+ * control for serving; no reference counterpart). */
+uint64_t cz_plane_bytes(const cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags);
+
+/* Free and total device memory of the handle's GPU (no reference counterpart). */
+int cz_mem_info(cz_handle *h, uint64_t *free_bytes, uint64_t *total_bytes);
+
+/* Device sieve for interval requests: for each i, the first count[i] primes
+ * >= lo[i] (fewer only where 2^32 is reached), written to out from slot
+ * sum(count[0..i-1]); found[i] = primes written.  Replaces the reference's
+ * bounded host sieve, src/census/prime_sieve.cpp:8-22. */
+int cz_sieve(cz_handle *h, const uint32_t *lo, const uint32_t *count, uint32_t n, uint32_t *out,
+             uint32_t *found);
 
 /* Quadratic A4 counts only (src/census/moment_worker.cpp:19-52 semantics):
  * x in [1, p-4] with x..x+3 all of one quadratic character; 0 for p = 2. */

@@ -26,7 +26,7 @@ class cz_config(ctypes.Structure):
     _fields_ = [("device", i32), ("sparse_min_p", u32), ("cover_n", u32), ("q_cap", u32 * 10),
                 ("anchor_bits", u32), ("screen", u32), ("sparse_blocks", u32), ("use_graph", u32),
                 ("cta_per_profile", u32), ("l1_carveout", u32), ("speculate", u32),
-                ("spec_margin10", u32 * 10), ("reserved", u32 * 3)]
+                ("spec_margin10", u32 * 10), ("plane_budget_mb", u32), ("reserved", u32 * 2)]
 
 
 class cz_stats(ctypes.Structure):
@@ -34,7 +34,7 @@ class cz_stats(ctypes.Structure):
                 ("ms_dense", ctypes.c_float), ("ms_a4", ctypes.c_float), ("ms_finalize", ctypes.c_float),
                 ("ms_device", ctypes.c_float), ("ms_h2d", ctypes.c_float), ("ms_d2h", ctypes.c_float),
                 ("n_primes", u32), ("n_dense", u32), ("n_sparse", u32), ("n_profiles", u32),
-                ("n_fallback", u32), ("n_respec", u32), ("ms_respec", ctypes.c_float),
+                ("n_fallback", u32), ("n_respec", u32), ("ms_respec", ctypes.c_float), ("waves", u32),
                 ("kernels", u32), ("words", u64), ("completions", u64),
                 ("tests", u64), ("h2d_bytes", u64), ("d2h_bytes", u64)]
 
@@ -43,7 +43,7 @@ class cz_stats(ctypes.Structure):
 
 
 EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_count_profiles",
-           "cz_census", "cz_replay", "cz_a4", "cz_microbench", "cz_census_dense_noalloc", "baseline_init",
+           "cz_census", "cz_replay", "cz_a4", "cz_sieve", "cz_plane_bytes", "cz_mem_info", "cz_microbench", "cz_census_dense_noalloc", "baseline_init",
            "baseline_profile"]
 
 _lib = None
@@ -76,6 +76,13 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.cz_replay.restype = ctypes.c_int
     L.cz_a4.argtypes = [H, ctypes.POINTER(u32), u32, ctypes.POINTER(u32)]
     L.cz_a4.restype = ctypes.c_int
+    L.cz_plane_bytes.argtypes = [H, ctypes.POINTER(u32), u32, u32]
+    L.cz_plane_bytes.restype = u64
+    L.cz_mem_info.argtypes = [H, ctypes.POINTER(u64), ctypes.POINTER(u64)]
+    L.cz_mem_info.restype = ctypes.c_int
+    L.cz_sieve.argtypes = [H, ctypes.POINTER(u32), ctypes.POINTER(u32), u32, ctypes.POINTER(u32),
+                           ctypes.POINTER(u32)]
+    L.cz_sieve.restype = ctypes.c_int
     L.cz_microbench.argtypes = [H, u32, ctypes.POINTER(ctypes.c_double)]
     L.cz_microbench.restype = ctypes.c_int
     L.cz_census_dense_noalloc.argtypes = [ctypes.POINTER(u32), u32, ctypes.POINTER(cz_profile), u32,

@@ -34,6 +34,7 @@ class Tuning:
     l1_carveout: int = 20
     speculate: int = 1
     spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 15, 15, 15, 15)
+    plane_budget_mb: int = 24 * 1024
 
 
 def _as_u32_array(values):
@@ -65,6 +66,7 @@ class Census:
         cfg.speculate = t.speculate
         for r in range(10):
             cfg.spec_margin10[r] = t.spec_margin10[r]
+        cfg.plane_budget_mb = t.plane_budget_mb
         h = ctypes.c_void_p()
         rc = self.lib.cz_open(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:
@@ -139,6 +141,34 @@ class Census:
         if rc != 0:
             raise CensusError(f"microbench failed (rc={rc}): {self._err()}")
         return v.value
+
+    def sieve(self, requests) -> list:
+        """Device sieve: for each (lo, count), the first `count` primes >= lo."""
+        n = len(requests)
+        lo = (ctypes.c_uint32 * max(1, n))(*[int(a) for a, _ in requests])
+        cnt = (ctypes.c_uint32 * max(1, n))(*[int(b) for _, b in requests])
+        total = sum(int(b) for _, b in requests)
+        out = (ctypes.c_uint32 * max(1, total))()
+        found = (ctypes.c_uint32 * max(1, n))()
+        rc = self.lib.cz_sieve(self.h, lo, cnt, n, out, found)
+        if rc != 0:
+            raise CensusError(f"sieve refused (rc={rc}): {self._err()}")
+        res, off = [], 0
+        for i in range(n):
+            res.append(list(out[off: off + found[i]]))
+            off += int(cnt[i])
+        return res
+
+    def plane_bytes(self, primes, mode: str = "auto") -> int:
+        arr = _as_u32_array(primes)
+        return int(self.lib.cz_plane_bytes(self.h, arr, len(primes), MODES[mode]))
+
+    def mem_info(self) -> tuple:
+        f, t = ctypes.c_uint64(), ctypes.c_uint64()
+        rc = self.lib.cz_mem_info(self.h, ctypes.byref(f), ctypes.byref(t))
+        if rc != 0:
+            raise CensusError(f"mem_info failed: {self._err()}")
+        return int(f.value), int(t.value)
 
     def a4(self, primes) -> list:
         n = len(primes)

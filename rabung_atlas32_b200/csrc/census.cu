@@ -26,6 +26,7 @@
 #include "finalize.cuh"
 #include "a4.cuh"
 #include "microbench.cuh"
+#include "sieve.cuh"
 #include "../../include/rabung_census.h"
 
 using namespace cz;
@@ -93,7 +94,7 @@ struct cz_handle {
     u32 n_small = 0;
     // device buffers
     Buf b_in, b_primes, b_profs, b_state, b_planes, b_summ, b_chunk, b_summp, b_didx, b_sidx,
-        b_slist, b_dlist, b_dpre, b_out, b_a4, b_counter;
+        b_slist, b_dlist, b_dpre, b_out, b_a4, b_counter, b_sreq, b_sout;
     // host copies of the current plan
     std::vector<PrimeDesc> hp;
     std::vector<ProfDesc> hprof;
@@ -492,6 +493,7 @@ int cz_default_config(cz_config *c) {
     c->cta_per_profile = 2;
     c->l1_carveout = 20;
     c->speculate = 1;
+    c->plane_budget_mb = 24u * 1024u;
     const u32 sm[10] = {0, 0, 30, 20, 15, 15, 15, 15, 15, 15};
     for (int r = 0; r < 10; ++r) c->spec_margin10[r] = sm[r];
     return CZ_OK;
@@ -516,6 +518,7 @@ int cz_open(const cz_config *cfg, cz_handle **out) {
     for (auto &e : h->ev) cudaEventCreate(&e);
     cudaFuncSetAttribute(table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_DYN_SMEM);
     cudaFuncSetAttribute(dense_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(sieve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SIEVE_MAX_WIDTH / 16 + 64);
     // the filter needs ~20 KB of shared memory per CTA: give the rest of the
     // unified L1/shared array to L1, where the colour planes are cached
     if (h->cfg.l1_carveout <= 100)
@@ -532,7 +535,7 @@ void cz_close(cz_handle *h) {
     if (h->graph) cudaGraphDestroy(h->graph);
     Buf *bufs[] = {&h->b_in, &h->b_primes, &h->b_profs, &h->b_state, &h->b_planes, &h->b_summ, &h->b_chunk,
                    &h->b_summp, &h->b_didx, &h->b_sidx, &h->b_slist, &h->b_dlist, &h->b_dpre, &h->b_out,
-                   &h->b_a4, &h->b_counter};
+                   &h->b_a4, &h->b_counter, &h->b_sreq, &h->b_sout};
     for (Buf *b : bufs) if (b->p) cudaFree(b->p);
     if (h->pin) cudaFreeHost(h->pin);
     if (h->d_small) cudaFree(h->d_small);
@@ -549,6 +552,61 @@ uint32_t cz_count_profiles(const uint32_t *primes, uint32_t n) {
     for (u32 i = 0; i < n; ++i)
         if (primes[i] > 2u) c += popc(mask_of(primes[i]));
     return c;
+}
+
+// plane-pool bytes one prime would take (0 for the dense route)
+static u64 plane_bytes(const cz_config &c, u32 p, u32 flags) {
+    if (p < 3u) return 0;
+    const u32 mode = flags & CZ_AUTO;
+    if (mode == CZ_DENSE || (mode == CZ_AUTO && p < c.sparse_min_p)) return 0;
+    const u32 mask = mask_of(p);
+    u32 Qmax = 0, units = 0;
+    for (u32 r = 2; r <= 9; ++r)
+        if (mask & (1u << (r - 2))) { Qmax = std::max(Qmax, q_for(c, r)); units += planes_stored(r); }
+    u32 B = 0;
+    if (Qmax + 1u >= p || !cover_B(p, Qmax, c.cover_n, B)) return 0;
+    const u64 words = (2ull * ((B + 31u) / 32u + 4u) + 8ull) + (2ull * ((B + 63u) / 64u + 4u) + 8ull);
+    return 4ull * words * units + 64ull * units;
+}
+
+static int census_impl(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags, cz_profile *out,
+                       uint32_t out_cap, uint32_t *a4_out, cz_stats *stats, bool allow_fallback);
+
+// a batch whose plane pool would exceed the budget runs as consecutive waves
+static int census_waves(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags, cz_profile *out,
+                        uint32_t out_cap, uint32_t *a4_out, cz_stats *stats) {
+    const u64 budget = (u64)h->cfg.plane_budget_mb << 20;
+    u64 acc = 0;
+    u32 start = 0, prof_off = 0, waves = 0;
+    cz_stats tot{};
+    for (u32 i = 0; i <= n; ++i) {
+        const u64 b = i < n ? plane_bytes(h->cfg, primes[i], flags) : 0;
+        if (i == n || (acc + b > budget && i > start)) {
+            const u32 m = i - start;
+            const u32 np = cz_count_profiles(primes + start, m);
+            cz_stats s{};
+            int rc = census_impl(h, primes + start, m, flags, out + prof_off, out_cap - prof_off,
+                                 a4_out ? a4_out + start : nullptr, &s, true);
+            if (rc) return rc;
+            ++waves;
+            tot.ms_setup += s.ms_setup; tot.ms_table += s.ms_table; tot.ms_sparse += s.ms_sparse;
+            tot.ms_dense += s.ms_dense; tot.ms_a4 += s.ms_a4; tot.ms_finalize += s.ms_finalize;
+            tot.ms_device += s.ms_device; tot.ms_h2d += s.ms_h2d; tot.ms_d2h += s.ms_d2h;
+            tot.n_dense += s.n_dense; tot.n_sparse += s.n_sparse; tot.n_profiles += s.n_profiles;
+            tot.n_fallback += s.n_fallback; tot.n_respec += s.n_respec; tot.ms_respec += s.ms_respec;
+            tot.kernels += s.kernels; tot.words += s.words; tot.completions += s.completions;
+            tot.tests += s.tests; tot.h2d_bytes += s.h2d_bytes; tot.d2h_bytes += s.d2h_bytes;
+            prof_off += np;
+            start = i;
+            acc = 0;
+        }
+        acc += b;
+    }
+    tot.n_primes = n;
+    tot.waves = waves;
+    h->have_plan = waves == 1 && h->have_plan;
+    if (stats) *stats = tot;
+    return CZ_OK;
 }
 
 static int census_impl(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags, cz_profile *out,
@@ -655,7 +713,35 @@ static int census_impl(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_
 
 int cz_census(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags, cz_profile *out,
               uint32_t out_cap, uint32_t *a4_out, cz_stats *stats) {
-    return census_impl(h, primes, n, flags, out, out_cap, a4_out, stats, true);
+    if (!h) return CZ_EINVAL;
+    if (n && primes && out && ((flags & CZ_A4) == 0 || a4_out)) {
+        if ((flags & CZ_AUTO) == 0) flags |= CZ_AUTO;
+        if (out_cap < cz_count_profiles(primes, n)) { h->err = "output capacity below profile count"; return CZ_EINVAL; }
+        u64 tot = 0;
+        for (u32 i = 0; i < n && tot <= ((u64)h->cfg.plane_budget_mb << 20); ++i) tot += plane_bytes(h->cfg, primes[i], flags);
+        if (tot > ((u64)h->cfg.plane_budget_mb << 20)) return census_waves(h, primes, n, flags, out, out_cap, a4_out, stats);
+    }
+    int rc = census_impl(h, primes, n, flags, out, out_cap, a4_out, stats, true);
+    if (!rc && stats) stats->waves = 1;
+    return rc;
+}
+
+uint64_t cz_plane_bytes(const cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags) {
+    if (!h || !primes) return 0;
+    if ((flags & CZ_AUTO) == 0) flags |= CZ_AUTO;
+    u64 t = 0;
+    for (u32 i = 0; i < n; ++i) t += plane_bytes(h->cfg, primes[i], flags);
+    return t;
+}
+
+int cz_mem_info(cz_handle *h, uint64_t *free_bytes, uint64_t *total_bytes) {
+    if (!h || !free_bytes || !total_bytes) return CZ_EINVAL;
+    cudaSetDevice(h->dev);
+    size_t f = 0, t = 0;
+    if (!ck(h, cudaMemGetInfo(&f, &t), "cudaMemGetInfo")) return CZ_ECUDA;
+    *free_bytes = f;
+    *total_bytes = t;
+    return CZ_OK;
 }
 
 int cz_replay(cz_handle *h, cz_stats *stats) {
@@ -694,6 +780,64 @@ int cz_replay(cz_handle *h, cz_stats *stats) {
     if (h->nprof) cudaMemcpy(h->hout.data(), h->b_out.p, sizeof(OutRecord) * h->nprof, cudaMemcpyDeviceToHost);
     if ((rc = check_records(h, nullptr))) return rc;
     if (stats) *stats = s;
+    return CZ_OK;
+}
+
+int cz_sieve(cz_handle *h, const uint32_t *lo, const uint32_t *count, uint32_t n, uint32_t *out,
+             uint32_t *found) {
+    if (!h || (n && (!lo || !count || !out || !found))) return CZ_EINVAL;
+    cudaSetDevice(h->dev);
+    h->err.clear();
+    if (n == 0) return CZ_OK;
+    std::vector<SieveReq> rq(n);
+    u64 total = 0;
+    for (u32 i = 0; i < n; ++i) {
+        rq[i] = SieveReq{};
+        rq[i].lo = lo[i];
+        rq[i].count = count[i];
+        rq[i].out_off = (u32)total;
+        total += count[i];
+        // prime number theorem with slack; widened below if a window comes up short
+        const double ln = std::log(std::max(16.0, (double)lo[i] + 1.0));
+        const u64 w = (u64)(count[i] * ln * 1.3) + 4096ull;
+        const u64 room = (1ull << 32) - lo[i];
+        rq[i].width = (u32)std::min<u64>({w, (u64)SIEVE_MAX_WIDTH, room});
+        found[i] = 0;
+    }
+    if (total > 0xFFFFFFFFull) { h->err = "sieve output too large"; return CZ_EINVAL; }
+    if (!ensure(h, h->b_sreq, sizeof(SieveReq) * n) || !ensure(h, h->b_sout, 4ull * std::max<u64>(1, total)))
+        return CZ_ECUDA;
+    std::vector<u32> todo(n);
+    for (u32 i = 0; i < n; ++i) todo[i] = i;
+    for (int round = 0; round < 24 && !todo.empty(); ++round) {
+        std::vector<SieveReq> sub;
+        for (u32 i : todo) sub.push_back(rq[i]);
+        cudaMemcpyAsync(h->b_sreq.p, sub.data(), sizeof(SieveReq) * sub.size(), cudaMemcpyHostToDevice, h->st);
+        const u32 grid = std::min<u32>((u32)sub.size(), (u32)h->sms);
+        sieve_kernel<<<grid, SIEVE_THREADS, SIEVE_MAX_WIDTH / 16 + 64, h->st>>>(P<SieveReq>(h->b_sreq), (u32)sub.size(),
+                                                                              h->d_small, h->n_small, P<u32>(h->b_sout));
+        cudaMemcpyAsync(sub.data(), h->b_sreq.p, sizeof(SieveReq) * sub.size(), cudaMemcpyDeviceToHost, h->st);
+        if (!ck(h, cudaStreamSynchronize(h->st), "sieve")) return CZ_ECUDA;
+        std::vector<u32> next;
+        for (size_t k = 0; k < todo.size(); ++k) {
+            SieveReq &R = rq[todo[k]];
+            R.found = sub[k].found;
+            const bool at_top = (u64)R.lo + R.width >= (1ull << 32);
+            if (R.found < R.count && !at_top) {
+                // too few primes in the window: widen it (the output slots are unchanged)
+                const u64 room = (1ull << 32) - R.lo;
+                const u64 w = std::min<u64>({(u64)R.width * 2ull, (u64)SIEVE_MAX_WIDTH, room});
+                if (w == R.width) { h->err = "sieve window limit reached"; return CZ_EINVAL; }
+                R.width = (u32)w;
+                next.push_back(todo[k]);
+            }
+        }
+        todo.swap(next);
+    }
+    if (!todo.empty()) { h->err = "sieve did not converge"; return CZ_EREFUSED; }
+    if (total && !ck(h, cudaMemcpy(out, h->b_sout.p, 4ull * total, cudaMemcpyDeviceToHost), "sieve d2h")) return CZ_ECUDA;
+    for (u32 i = 0; i < n; ++i) found[i] = rq[i].found;
+    h->have_plan = false;
     return CZ_OK;
 }
 

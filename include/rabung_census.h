@@ -68,7 +68,8 @@ typedef struct cz_config {
     uint32_t speculate;      /* 1: speculative thresholds floor(log_r p - margin), re-run on a miss */
     uint32_t spec_margin10[10];  /* margin per order r, in tenths */
     uint32_t plane_budget_mb;    /* plane pool per wave; larger batches run as consecutive waves */
-    uint32_t reserved[2];
+    uint32_t dense_steps;        /* dense scan segment: 32 x dense_steps values of x per warp */
+    uint32_t reserved[1];
 } cz_config;
 
 typedef struct cz_stats {
@@ -112,6 +113,10 @@ int cz_replay(cz_handle *h, cz_stats *stats);
 /* Device memory the colour planes of these primes would take (admission
  * control for serving; no reference counterpart). */
 uint64_t cz_plane_bytes(const cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t flags);
+
+/* Name and SM count of the handle's GPU (keys the autotuner's saved choices;
+ * no reference counterpart). */
+int cz_device_info(cz_handle *h, char *name, uint32_t len, uint32_t *sms);
 
 /* Free and total device memory of the handle's GPU (no reference counterpart). */
 int cz_mem_info(cz_handle *h, uint64_t *free_bytes, uint64_t *total_bytes);

@@ -26,7 +26,8 @@ class cz_config(ctypes.Structure):
     _fields_ = [("device", i32), ("sparse_min_p", u32), ("cover_n", u32), ("q_cap", u32 * 10),
                 ("anchor_bits", u32), ("screen", u32), ("sparse_blocks", u32), ("use_graph", u32),
                 ("cta_per_profile", u32), ("l1_carveout", u32), ("speculate", u32),
-                ("spec_margin10", u32 * 10), ("plane_budget_mb", u32), ("reserved", u32 * 2)]
+                ("spec_margin10", u32 * 10), ("plane_budget_mb", u32), ("dense_steps", u32),
+                ("reserved", u32 * 1)]
 
 
 class cz_stats(ctypes.Structure):
@@ -43,7 +44,8 @@ class cz_stats(ctypes.Structure):
 
 
 EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_count_profiles",
-           "cz_census", "cz_replay", "cz_a4", "cz_sieve", "cz_plane_bytes", "cz_mem_info", "cz_microbench", "cz_census_dense_noalloc", "baseline_init",
+           "cz_census", "cz_replay", "cz_a4", "cz_sieve", "cz_plane_bytes", "cz_mem_info", "cz_device_info",
+           "cz_microbench", "cz_census_dense_noalloc", "baseline_init",
            "baseline_profile"]
 
 _lib = None
@@ -78,6 +80,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.cz_a4.restype = ctypes.c_int
     L.cz_plane_bytes.argtypes = [H, ctypes.POINTER(u32), u32, u32]
     L.cz_plane_bytes.restype = u64
+    L.cz_device_info.argtypes = [H, ctypes.c_char_p, u32, ctypes.POINTER(u32)]
+    L.cz_device_info.restype = ctypes.c_int
     L.cz_mem_info.argtypes = [H, ctypes.POINTER(u64), ctypes.POINTER(u64)]
     L.cz_mem_info.restype = ctypes.c_int
     L.cz_sieve.argtypes = [H, ctypes.POINTER(u32), ctypes.POINTER(u32), u32, ctypes.POINTER(u32),

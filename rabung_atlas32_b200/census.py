@@ -35,6 +35,7 @@ class Tuning:
     speculate: int = 1
     spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 15, 15, 15, 15)
     plane_budget_mb: int = 24 * 1024
+    dense_steps: int = 256
 
 
 def _as_u32_array(values):
@@ -47,11 +48,28 @@ def _as_u32_array(values):
 
 
 class Census:
-    def __init__(self, device: int = 0, tuning: Tuning | None = None):
+    def __init__(self, device: int = 0, tuning: Tuning | None = None, autoload: bool = True):
+        """Open a handle on `device`.  Without an explicit tuning, the
+        autotuner's saved choices for this GPU (rabung_atlas32_b200/tuned/) are
+        used when present."""
         self.lib = _lib.load()
+        self.h = None
+        self.tuned_from = None
+        if tuning is None and autoload:
+            self._open(device, Tuning())
+            from .autotune import device_key, load_tuned
+            key = device_key(self)
+            t = load_tuned(key)
+            if t is None:
+                return
+            self.close()
+            self.tuned_from = key
+            tuning = t
+        self._open(device, tuning or Tuning())
+
+    def _open(self, device: int, t: Tuning):
         cfg = _lib.cz_config()
         self.lib.cz_default_config(ctypes.byref(cfg))
-        t = tuning or Tuning()
         cfg.device = device
         cfg.sparse_min_p = t.sparse_min_p
         cfg.cover_n = t.cover_n
@@ -67,11 +85,13 @@ class Census:
         for r in range(10):
             cfg.spec_margin10[r] = t.spec_margin10[r]
         cfg.plane_budget_mb = t.plane_budget_mb
+        cfg.dense_steps = t.dense_steps
         h = ctypes.c_void_p()
         rc = self.lib.cz_open(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:
             raise CensusError(f"cz_open failed (rc={rc}): no usable CUDA device or bad tuning")
         self.h = h
+        self.tuning = t
         self.last_stats: dict = {}
 
     def close(self):

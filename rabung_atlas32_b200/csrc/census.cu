@@ -163,6 +163,12 @@ bool build_static_tables(cz_handle *h) {
 
 u32 q_for(const cz_config &c, u32 r) { return c.q_cap[r] ? c.q_cap[r] : 16u; }
 
+// dense segment length in x (32 x steps), default DENSE_SEG
+u32 dense_seg(const cz_config &c) {
+    const u32 steps = c.dense_steps ? std::min(4096u, std::max(8u, c.dense_steps)) : (u32)DENSE_STEPS;
+    return 32u * steps;
+}
+
 // speculative threshold: floor(log_r p - margin_r), a low quantile of M for
 // random-looking colourings (M ~ log_r p); 0 disables
 u32 qspec_for(const cz_config &c, u32 p, u32 r, bool allow) {
@@ -231,7 +237,8 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
             max_slots_t = std::max(max_slots_t, hash_slots(P.m));
         } else {
             const u32 nh = (p - 1u) / 2u;
-            const u32 nseg = (nh + DENSE_SEG - 1u) / DENSE_SEG;
+            const u32 seg = dense_seg(c);
+            const u32 nseg = (nh + seg - 1u) / seg;
             const u32 nch = (nseg + DENSE_WARPS - 1u) / DENSE_WARPS;
             h->h_didx.push_back(i);
             h->h_summp.push_back((u32)summ_slots);
@@ -411,6 +418,7 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
         da.nchunks = h->nchunks;
         da.summ = P<Summ>(h->b_summ);
         da.state = P<ProfState>(h->b_state);
+        da.seg = dense_seg(h->cfg);
         const u32 grid = std::min<u32>(h->nchunks, (u32)h->sms * 8u);
         dense_scan_kernel<<<grid, DENSE_WARPS * 32, h->dense_smem, st>>>(da);
         DenseMergeArgs ma;
@@ -494,6 +502,7 @@ int cz_default_config(cz_config *c) {
     c->l1_carveout = 20;
     c->speculate = 1;
     c->plane_budget_mb = 24u * 1024u;
+    c->dense_steps = DENSE_STEPS;
     const u32 sm[10] = {0, 0, 30, 20, 15, 15, 15, 15, 15, 15};
     for (int r = 0; r < 10; ++r) c->spec_margin10[r] = sm[r];
     return CZ_OK;
@@ -732,6 +741,15 @@ uint64_t cz_plane_bytes(const cz_handle *h, const uint32_t *primes, uint32_t n, 
     u64 t = 0;
     for (u32 i = 0; i < n; ++i) t += plane_bytes(h->cfg, primes[i], flags);
     return t;
+}
+
+int cz_device_info(cz_handle *h, char *name, uint32_t len, uint32_t *sms) {
+    if (!h || !name || !len || !sms) return CZ_EINVAL;
+    cudaDeviceProp prop;
+    if (!ck(h, cudaGetDeviceProperties(&prop, h->dev), "device properties")) return CZ_ECUDA;
+    snprintf(name, len, "%s", prop.name);
+    *sms = (uint32_t)prop.multiProcessorCount;
+    return CZ_OK;
 }
 
 int cz_mem_info(cz_handle *h, uint64_t *free_bytes, uint64_t *total_bytes) {
@@ -1036,6 +1054,7 @@ extern "C" int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_pr
     da.nchunks = chunk[nd];
     da.summ = reinterpret_cast<Summ *>(base + L.summ);
     da.state = dS;
+    da.seg = DENSE_SEG;
     dense_scan_kernel<<<std::max(1u, std::min(chunk[nd], 1184u)), DENSE_WARPS * 32, max_slots * 6u + 16u, st>>>(da);
     DenseMergeArgs ma;
     ma.primes = dP;

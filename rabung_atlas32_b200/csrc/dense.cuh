@@ -68,6 +68,7 @@ struct DenseArgs {
     u32 nchunks;                   // total chunks
     Summ *summ;                    // per prime: nprof x nchunks chunk summaries, profile-major
     ProfState *state;
+    u32 seg;                       // x per segment (a multiple of 32; DENSE_SEG by default)
 };
 
 // One CTA per (prime, chunk of DENSE_WARPS segments); one warp per segment.
@@ -103,7 +104,7 @@ dense_scan_kernel(DenseArgs a) {
         const u32 local_chunk = chunk - a.chunk_prefix[pi];
         const u32 nh = (P.p - 1u) >> 1;
         const u32 seg = local_chunk * DENSE_WARPS + warp;
-        const u32 seg_start = 1u + seg * DENSE_SEG;          // x of the first element
+        const u32 seg_start = 1u + seg * a.seg;              // x of the first element
         const u32 nprof = P.nprof;
         // per-profile warp-uniform state
         u32 rr[8], mg[8], carry_c[8], carry_start[8], carry_len[8], pre[8], bl[8], bs[8], cf[8];
@@ -117,7 +118,7 @@ dense_scan_kernel(DenseArgs a) {
         }
         u32 lastc[8];
         bool active = seg_start <= nh;
-        u32 seg_end = active ? min(nh, seg_start + DENSE_SEG - 1u) : 0u;   // inclusive
+        u32 seg_end = active ? min(nh, seg_start + a.seg - 1u) : 0u;   // inclusive
         u32 bad = 0;
         if (active) {
             const u32 nsteps = (seg_end - seg_start) / 32u + 1u;

@@ -26,7 +26,7 @@ def test_header_symbols_exported():
 def test_struct_layouts():
     from rabung_atlas32_b200 import _lib
     assert ctypes.sizeof(_lib.cz_profile) == 32
-    assert ctypes.sizeof(_lib.cz_config) == 4 * (1 + 1 + 1 + 10 + 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 2)
+    assert ctypes.sizeof(_lib.cz_config) == 4 * (1 + 1 + 1 + 10 + 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 1)
 
 
 def test_count_profiles_host_only():

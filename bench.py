@@ -94,6 +94,38 @@ def uneven_arm(args) -> None:
         "batched_over_plain": round(plain_dev / (sum(dev) / len(dev)), 3), "bit_identical": same}))
 
 
+def max_over_ranks(values: list, dist=None, device=None) -> list:
+    """Element-wise maximum of per-rank timings (every rank gets the result)."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def small_arm(args) -> None:
+    """C1 (first 256 primes, dense) and C2 (4096 primes from 2^24, dense oracle
+    and anchor filter) timings."""
+    from rabung_atlas32_b200 import sieve
+    from rabung_atlas32_b200.census import Census
+    eng = Census()
+    res = {}
+    for name, ps, mode in (("C1_first_256_dense", sieve.primes_from(2, 256), "dense"),
+                           ("C2_2p24_dense", sieve.primes_from(1 << 24, BLOCK), "dense"),
+                           ("C2_2p24_sparse", sieve.primes_from(1 << 24, BLOCK), "sparse")):
+        for _ in range(args.warmup):
+            eng.raw(ps, mode=mode, a4=True)
+        ms = []
+        for _ in range(args.steps):
+            _, _, st = eng.raw(ps, mode=mode, a4=True)
+            ms.append(st["ms_device"])
+        n = eng.count_profiles(ps)
+        res[name] = {"profiles": n, "ms_device": round(sum(ms) / len(ms), 3),
+                     "profiles_per_s": round(n / (sum(ms) / len(ms) / 1000.0), 1)}
+    print(json.dumps({"metric": "profiles/s, C1 and C2 blocks", "results": res}))
+
+
 def workload(rank: int) -> list:
     from rabung_atlas32_b200 import sieve
     hi = TOP
@@ -229,7 +261,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="top", choices=["top", "uneven", "serve"])
+    ap.add_argument("--workload", default="top", choices=["top", "uneven", "serve", "small"])
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--rate", type=float, default=40.0, help="offered load, requests/s (serve)")
     args = ap.parse_args()
@@ -240,6 +272,9 @@ def main():
         return
     if args.workload == "uneven":
         uneven_arm(args)
+        return
+    if args.workload == "small":
+        small_arm(args)
         return
     if args.workload == "serve":
         from rabung_atlas32_b200 import serving
@@ -301,10 +336,7 @@ def main():
         h2d, d2h = st["h2d_bytes"], st["d2h_bytes"]
     barrier()
     e2e_total = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([total_ms, e2e_total], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_total = float(t[0]), float(t[1])
+    total_ms, e2e_total = max_over_ranks([total_ms, e2e_total], dist, f"cuda:{local}")
     value = world * nprof * args.steps / (total_ms / 1000.0)
     e2e_value = world * nprof * args.steps / (e2e_total / 1000.0)
 

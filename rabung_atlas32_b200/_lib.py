@@ -7,6 +7,7 @@ fallback in the product path.
 from __future__ import annotations
 
 import ctypes
+import os
 from pathlib import Path
 
 from .build import LIB
@@ -56,7 +57,7 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB
+    p = Path(path) if path else Path(os.environ.get("RABUNG_CENSUS_LIB", str(LIB)))
     if not p.exists():
         raise OSError(f"{p} is not built; run `python -m rabung_atlas32_b200.build`")
     L = ctypes.CDLL(str(p))

@@ -44,6 +44,22 @@
 
 namespace cz {
 
+#ifndef CZ_SB1                       // anchor stages whose loads issue together, by stored planes
+#define CZ_SB1 4
+#endif
+#ifndef CZ_SB2
+#define CZ_SB2 2
+#endif
+#ifndef CZ_SB4
+#define CZ_SB4 1
+#endif
+#ifndef CZ_SPARSE_MINB                // resident filter CTAs per SM (register budget)
+#define CZ_SPARSE_MINB 2
+#endif
+#ifndef CZ_WORD64                     // 1: 64 anchors per lane-word, 0: 32
+#define CZ_WORD64 1
+#endif
+
 constexpr int SPARSE_WARPS = 16;
 constexpr int CAND_CAP = 64;          // per-warp buffers
 constexpr u32 RUN_CAP = 4096;         // longest run a completion may walk
@@ -84,6 +100,13 @@ template <> struct Planes<1> {
         const u32 *q = P + (u >> 5);
         o[0] = __funnelshift_r(__ldg(q), __ldg(q + 1), u & 31u);
     }
+    // 64-bit window: lo = bits [u, u+32), hi = bits [u+32, u+64)
+    static __device__ __forceinline__ void win64(const u32 *__restrict__ P, u32 u, u32 *lo, u32 *hi) {
+        const u32 *q = P + (u >> 5);
+        const u32 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), sh = u & 31u;
+        lo[0] = __funnelshift_r(a, b, sh);
+        hi[0] = __funnelshift_r(b, c, sh);
+    }
 };
 template <> struct Planes<2> {
     static __device__ __forceinline__ void win(const u32 *__restrict__ P, u32 u, u32 *o) {
@@ -91,6 +114,13 @@ template <> struct Planes<2> {
         const uint2 a = __ldg(q), b = __ldg(q + 1);
         o[0] = __funnelshift_r(a.x, b.x, u & 31u);
         o[1] = __funnelshift_r(a.y, b.y, u & 31u);
+    }
+    static __device__ __forceinline__ void win64(const u32 *__restrict__ P, u32 u, u32 *lo, u32 *hi) {
+        const uint2 *q = reinterpret_cast<const uint2 *>(P) + (u >> 5);
+        const uint2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+        const u32 sh = u & 31u;
+        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
+        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
     }
 };
 template <> struct Planes<4> {
@@ -103,6 +133,15 @@ template <> struct Planes<4> {
         o[2] = __funnelshift_r(a.z, b.z, sh);
         o[3] = __funnelshift_r(a.w, b.w, sh);
     }
+    static __device__ __forceinline__ void win64(const u32 *__restrict__ P, u32 u, u32 *lo, u32 *hi) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(P) + (u >> 5);
+        const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+        const u32 sh = u & 31u;
+        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
+        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
+        lo[2] = __funnelshift_r(a.z, b.z, sh); hi[2] = __funnelshift_r(b.z, c.z, sh);
+        lo[3] = __funnelshift_r(a.w, b.w, sh); hi[3] = __funnelshift_r(b.w, c.w, sh);
+    }
 };
 
 // mismatch mask of a window against the base windows
@@ -114,6 +153,17 @@ __device__ __forceinline__ u32 mismatch(const u32 *__restrict__ P, u32 u, const 
 #pragma unroll
     for (int k = 1; k < NPP; ++k) m |= w[k] ^ base[k];
     return m;
+}
+
+// 64-bit mismatch mask (hi:lo) of a window against the base windows
+template <int NPP>
+__device__ __forceinline__ u64 mismatch64(const u32 *__restrict__ P, u32 u, const u32 *blo, const u32 *bhi) {
+    u32 lo[NPP], hi[NPP];
+    Planes<NPP>::win64(P, u, lo, hi);
+    u32 ml = lo[0] ^ blo[0], mh = hi[0] ^ bhi[0];
+#pragma unroll
+    for (int k = 1; k < NPP; ++k) { ml |= lo[k] ^ blo[k]; mh |= hi[k] ^ bhi[k]; }
+    return ((u64)mh << 32) | ml;
 }
 
 // one view of the signed table: index i <-> numerator c + G i, i in [ilo, ihi]
@@ -329,7 +379,7 @@ __device__ __forceinline__ void filter_row(const ProfCtx &c, const View &vref, u
             Planes<NPP>::win(v.P, u, bw);
             // stages in batches of SB: the batch's window loads are independent and
             // issue back to back, so their latency is paid once per batch
-            constexpr int SB = NPP == 4 ? 2 : 4;
+            constexpr int SB = NPP == 4 ? CZ_SB4 : (NPP == 2 ? CZ_SB2 : CZ_SB1);
             u32 j = 1;
             while (j < t && alive) {
                 u32 m[SB];
@@ -357,7 +407,85 @@ __device__ __forceinline__ void filter_row(const ProfCtx &c, const View &vref, u
         screen_batch<NPP>(c, v, sb, cb, q, q.nscr, d, dd, t, h, tune.screen != 0u, dinv, have_inv, st, lane);
 }
 
-__global__ void __launch_bounds__(SPARSE_WARPS * 32, 2)
+// queue one 32-bit half-word per lane for the batched screen (the batch runs
+// as soon as 32 are waiting)
+template <int NPP>
+__device__ __forceinline__ void queue_words(const ProfCtx &c, const View &v, uint2 *sb, Cand *cb, WarpQ &q,
+                                            u32 i0, u32 alive, u32 d, u32 dd, u32 t, u32 h, bool screen,
+                                            u32 &dinv, bool &have_inv, ProfState *st, int lane) {
+    const bool has = alive != 0u;
+    const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
+    if (!bal) return;
+    const u32 pos = __popc(bal & ((1u << lane) - 1u));
+    if (has) sb[q.nscr + pos] = make_uint2(i0, alive);
+    q.nscr += __popc(bal);
+    __syncwarp();
+    if (q.nscr >= 32u) screen_batch<NPP>(c, v, sb, cb, q, 32u, d, dd, t, h, screen, dinv, have_inv, st, lane);
+}
+
+// all selected words of row d on view v, 64 anchors per lane-word: per stage
+// three plane words, two funnel shifts and two logic ops per plane test 64
+// anchors, so ALU work and L1 requests per anchor-stage drop against 32-bit
+// words for a few more stages per word
+template <int NPP>
+__device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref, u32 d, u32 t, u32 s, u32 h,
+                                             const Tuning &tune, uint2 *sb, Cand *cb, WarpQ &q, ProfState *st,
+                                             int lane) {
+    const View v = vref;
+    const u32 G = v.G, dd = d / G;
+    const u32 beta = ((t - 1u) * d + 1u) >> 1;
+    const i32 istart = (i32)((beta >= v.c ? beta - v.c + G - 1u : 0u) / G);
+    if (istart > v.ihi) return;
+    const u32 step = dd * s;
+    const u32 K = (u32)(v.ihi - istart) / step + 1u;
+    const u32 nw = (dd + 63u) >> 6;
+    const u32 W = K * nw;
+    const float rnw = 1.0f / (float)nw;
+    const bool screen = tune.screen != 0u;
+    u32 dinv = 0;
+    bool have_inv = false;
+    for (u32 base = 0; base < W; base += 32u) {
+        const u32 rank = base + (u32)lane;
+        u64 alive = 0;
+        u32 i0 = 0;
+        if (rank < W) {
+            u32 k = (u32)((float)rank * rnw);
+            if (k * nw > rank) --k;
+            else if ((k + 1u) * nw <= rank) ++k;
+            const u32 w = rank - k * nw;
+            i0 = (u32)istart + k * step + 64u * w;
+            u32 len = dd - 64u * w;
+            if (len > 64u) len = 64u;
+            if ((i32)i0 > v.ihi) len = 0;
+            else if ((u32)(v.ihi - (i32)i0) + 1u < len) len = (u32)(v.ihi - (i32)i0) + 1u;
+            alive = len >= 64u ? ~0ull : ((1ull << len) - 1ull);
+        }
+        if (alive) {
+            ++q.words;
+            const u32 u = i0 + v.OFF;
+            u32 blo[NPP], bhi[NPP];
+            Planes<NPP>::win64(v.P, u, blo, bhi);
+            constexpr int SB = NPP == 4 ? CZ_SB4 : (NPP == 2 ? CZ_SB2 : CZ_SB1);
+            u32 j = 1;
+            while (j < t && alive) {
+                u64 m[SB];
+#pragma unroll
+                for (int k = 0; k < SB; ++k)
+                    m[k] = (j + (u32)k < t) ? mismatch64<NPP>(v.P, u - (j + (u32)k) * dd, blo, bhi) : 0ull;
+#pragma unroll
+                for (int k = 0; k < SB; ++k) alive &= ~m[k];
+                j += SB;
+            }
+            q.tests += 2u * min(j, t) * (u32)NPP;
+        }
+        queue_words<NPP>(c, v, sb, cb, q, i0, (u32)alive, d, dd, t, h, screen, dinv, have_inv, st, lane);
+        queue_words<NPP>(c, v, sb, cb, q, i0 + 32u, (u32)(alive >> 32), d, dd, t, h, screen, dinv, have_inv, st,
+                         lane);
+    }
+    if (q.nscr) screen_batch<NPP>(c, v, sb, cb, q, q.nscr, d, dd, t, h, screen, dinv, have_inv, st, lane);
+}
+
+__global__ void __launch_bounds__(SPARSE_WARPS * 32, CZ_SPARSE_MINB)
 sparse_kernel(SparseArgs a) {
     __shared__ u32 s_item, s_err, s_qspec;
     __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];      // candidates awaiting completion
@@ -415,9 +543,15 @@ sparse_kernel(SparseArgs a) {
             const u32 s = q_ - t + 1u;
             const u32 h = blen > t ? blen - t : 0u;      // screen: reject runs certified < blen
             const View &v = (d & 1u) ? c.base : c.odd;
+#if CZ_WORD64
+            if (c.npp == 1u) filter_row64<1>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
+            else if (c.npp == 2u) filter_row64<2>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
+            else filter_row64<4>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
+#else
             if (c.npp == 1u) filter_row<1>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
             else if (c.npp == 2u) filter_row<2>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
             else filter_row<4>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
+#endif
         }
         if (q.ncand) flush_cands(c, cb, q, q.ncand, st, lane);
         if (q.err) atomicOr(&s_err, q.err);

@@ -133,21 +133,39 @@ table_kernel(TableArgs a) {
         for (u32 ks = k0; ks < k1; ks += TABLE_SUB) {
             const u32 ke = min(k1, ks + TABLE_SUB);
             const bool need_pre = (ks == k0 && k0 > 0);
-            // stage labels of steps [ks - need_pre, ke)
-            for (u32 k = ks - (need_pre ? 1u : 0u); k < ke; ++k) {
-                const u32 n = 32u * k + (u32)lane;
-                u32 l = 0;
-                if (n >= 2u && n < a.chain_limit) {
-                    u32 v = n;
-                    for (int g = 0; g < 24 && v > 1u; ++g) {
-                        const uint2 c = a.chain[v];
-                        l += plab[c.x];
-                        v = c.y;
-                    }
-                    if (v > 1u) bad = 1;
-                    l = mod_small(l, P.m, magic_of(P.m));
+            // stage labels of steps [ks - need_pre, ke): the TABLE_SUB + 1 chains of
+            // a lane are walked in lockstep, so their dependent loads overlap
+            {
+                const u32 kfirst = ks - (need_pre ? 1u : 0u);
+                u32 v[TABLE_SUB + 1], l[TABLE_SUB + 1];
+#pragma unroll
+                for (u32 i = 0; i <= TABLE_SUB; ++i) {
+                    const u32 k = kfirst + i;
+                    const u32 n = 32u * k + (u32)lane;
+                    v[i] = (k < ke && n >= 2u && n < a.chain_limit) ? n : 1u;
+                    l[i] = 0u;
                 }
-                lab[warp][k + 1u - ks][lane] = (unsigned short)l;   // slot 0 = pre-step
+                for (int g = 0; g < 24; ++g) {
+                    bool any = false;
+#pragma unroll
+                    for (u32 i = 0; i <= TABLE_SUB; ++i) {
+                        if (v[i] > 1u) {
+                            const uint2 c = a.chain[v[i]];
+                            l[i] += plab[c.x];
+                            v[i] = c.y;
+                            any = true;
+                        }
+                    }
+                    if (!any) break;
+                }
+                const u32 mgm = magic_of(P.m);
+#pragma unroll
+                for (u32 i = 0; i <= TABLE_SUB; ++i) {
+                    const u32 k = kfirst + i;
+                    if (k >= ke) break;
+                    if (v[i] > 1u) bad = 1;
+                    lab[warp][k + 1u - ks][lane] = (unsigned short)mod_small(l[i], P.m, mgm);   // slot 0 = pre-step
+                }
             }
             __syncwarp();
             for (u32 s = 0; s < nprof; ++s) {

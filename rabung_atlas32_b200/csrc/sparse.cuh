@@ -37,8 +37,8 @@
 // maximum at every row, so the threshold rises while the profile runs; lanes
 // take consecutive words of a row (one vector load fetches all interleaved
 // planes of a word, funnel shifts cut the windows); words that survive the
-// anchor are queued per warp and screened 32 at a time, one per lane, and the
-// screened candidates are completed 32 at a time, one per lane.
+// anchor are queued per warp (across rows) and screened 32 at a time, one per
+// lane, and the screened candidates are completed 32 at a time, one per lane.
 #pragma once
 #include "labels.cuh"
 
@@ -55,9 +55,6 @@ namespace cz {
 #endif
 #ifndef CZ_SPARSE_MINB                // resident filter CTAs per SM (register budget)
 #define CZ_SPARSE_MINB 2
-#endif
-#ifndef CZ_WORD64                     // 1: 64 anchors per lane-word, 0: 32
-#define CZ_WORD64 1
 #endif
 
 constexpr int SPARSE_WARPS = 16;
@@ -81,7 +78,7 @@ struct SparseArgs {
     Tuning tune;
 };
 
-struct Cand { u32 b, d, dinv; };
+struct Cand { u32 b, d; };
 
 // preferred anchor length: least t with r^(t-1) >= 2^(5+bits), i.e. a word of
 // 32 random anchors keeps on average <= 2^-bits survivors
@@ -180,6 +177,7 @@ struct ProfCtx {
     const u32 *P;          // base view planes
     View base, odd;
     u32 om[9];
+    u32 seed, qspec;       // certified stretch from the table, speculative threshold
 };
 
 // colour of numerator n (|n| <= B) as an integer, from the base view
@@ -200,9 +198,11 @@ __device__ __forceinline__ u32 colour_direct(u32 x, const ProfCtx &c) {
 
 // exact completion of one candidate; returns packed key (0 on reject) and
 // sets *err on an arithmetic failure
-__device__ __noinline__ u64 complete_one(const ProfCtx &c, u32 b, u32 d, u32 dinv, u32 *err) {
+__device__ __noinline__ u64 complete_one(const ProfCtx &c, u32 b, u32 d, u32 *err) {
     const u32 p = c.p;
-    const u32 xr = mmul(b, dinv, c.M);                 // b * d^-1 mod p (dinv in Montgomery form)
+    // Montgomery d^-1 (= R d^-1), so mmul(b, dinv) = b d^-1 mod p
+    const u32 dinv = mpow(to_mont(d, c.M), c.p - 2u, c.M);
+    const u32 xr = mmul(b, dinv, c.M);
     if (xr == 0u) return 0;
     const u32 cb = colour_at(c, b + c.OFF);
     const u32 cd = colour_at(c, d + c.OFF);
@@ -286,7 +286,7 @@ __device__ __forceinline__ void flush_cands(const ProfCtx &c, Cand *cb, WarpQ &q
     if ((u32)lane < count) {
         const Cand cd = cb[lane];
         u32 e = 0;
-        key = complete_one(c, cd.b, cd.d, cd.dinv, &e);
+        key = complete_one(c, cd.b, cd.d, &e);
         q.err |= e;
     }
     q.comps += count;
@@ -302,36 +302,46 @@ __device__ __forceinline__ void flush_cands(const ProfCtx &c, Cand *cb, WarpQ &q
     if (lane == 0 && q.best) atomicMax(&st->best, (unsigned long long)q.best);
 }
 
-// screen `count` (<= 32) queued words of the current row and queue the
-// surviving candidates for completion
+// current threshold of the profile: the verified maximum (<= M), raised to the
+// speculative threshold when one is set
+__device__ __forceinline__ u32 threshold(const ProfCtx &c, ProfState *st) {
+    const u64 bk = *(volatile unsigned long long *)&st->best;
+    const u32 blen = key_len(bk) > c.seed ? key_len(bk) : c.seed;
+    return c.qspec > blen ? c.qspec : blen;
+}
+
+// screen `count` (<= 32) queued words -- one per lane, each remembering its row
+// (d, t) -- and queue the surviving candidates for completion; the queue is
+// carried across rows, so batches stay full
 template <int NPP>
-__device__ __forceinline__ void screen_batch(const ProfCtx &c, const View &v, uint2 *sb, Cand *cb, WarpQ &q,
-                                             u32 count, u32 d, u32 dd, u32 t, u32 h, bool screen, u32 &dinv,
-                                             bool &have_inv, ProfState *st, int lane) {
-    u32 keep = 0, i0 = 0;
+__device__ __forceinline__ void screen_batch(const ProfCtx &c, uint4 *sb, Cand *cb, WarpQ &q, u32 count,
+                                             bool screen, ProfState *st, int lane) {
+    u32 keep = 0, i0 = 0, d = 0, vc = 0, vg = 1;
+    const u32 thr = threshold(c, st);
     if ((u32)lane < count) {
-        const uint2 e = sb[lane];
+        const uint4 e = sb[lane];
         i0 = e.x;
         keep = e.y;
-        if (screen && h > 0u) keep = screen_word<NPP>(v, i0, keep, dd, t, h);
+        d = e.z;
+        const u32 t = e.w;
+        const View &v = (d & 1u) ? c.base : c.odd;
+        vc = v.c;
+        vg = v.G;
+        const u32 h = thr > t ? thr - t : 0u;     // reject runs certified < threshold
+        if (screen && h > 0u) keep = screen_word<NPP>(v, i0, keep, d / v.G, t, h);
     }
     __syncwarp();
     if (q.nscr > count && (u32)lane < q.nscr - count) sb[lane] = sb[count + lane];
     __syncwarp();
     q.nscr -= count;
     while (__any_sync(0xFFFFFFFFu, keep != 0u)) {
-        if (!have_inv) {
-            // Montgomery d^-1 (= R d^-1), so mmul(b, dinv) = b d^-1 mod p
-            dinv = mpow(to_mont(d, c.M), c.p - 2u, c.M);
-            have_inv = true;
-        }
         const bool has = keep != 0u;
         const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
         const u32 pos = __popc(bal & ((1u << lane) - 1u));
         if (has) {
             const u32 bit = __ffs(keep) - 1u;
             keep &= keep - 1u;
-            cb[q.ncand + pos] = Cand{v.c + v.G * (i0 + bit), d, dinv};
+            cb[q.ncand + pos] = Cand{vc + vg * (i0 + bit), d};
         }
         q.ncand += __popc(bal);
         __syncwarp();
@@ -339,88 +349,19 @@ __device__ __forceinline__ void screen_batch(const ProfCtx &c, const View &v, ui
     }
 }
 
-// all selected words of row d on view v (anchor filter, queue, screen, complete)
-template <int NPP>
-__device__ __forceinline__ void filter_row(const ProfCtx &c, const View &vref, u32 d, u32 t, u32 s, u32 h,
-                                           const Tuning &tune, uint2 *sb, Cand *cb, WarpQ &q, ProfState *st,
-                                           int lane) {
-    const View v = vref;
-    const u32 G = v.G, dd = d / G;
-    const u32 beta = ((t - 1u) * d + 1u) >> 1;
-    // first view index of band 0: least i with c + G i >= beta
-    const i32 istart = (i32)((beta >= v.c ? beta - v.c + G - 1u : 0u) / G);
-    if (istart > v.ihi) return;
-    const u32 step = dd * s;                       // band period in view indices
-    const u32 K = (u32)(v.ihi - istart) / step + 1u;
-    const u32 nw = (dd + 31u) >> 5;
-    const u32 W = K * nw;
-    const float rnw = 1.0f / (float)nw;
-    u32 dinv = 0;
-    bool have_inv = false;
-    for (u32 base = 0; base < W; base += 32u) {
-        const u32 rank = base + (u32)lane;
-        u32 alive = 0, i0 = 0;
-        if (rank < W) {
-            u32 k = (u32)((float)rank * rnw);
-            if (k * nw > rank) --k;
-            else if ((k + 1u) * nw <= rank) ++k;
-            const u32 w = rank - k * nw;
-            i0 = (u32)istart + k * step + 32u * w;
-            u32 len = dd - 32u * w;
-            if (len > 32u) len = 32u;
-            if ((i32)i0 > v.ihi) len = 0;
-            else if ((u32)(v.ihi - (i32)i0) + 1u < len) len = (u32)(v.ihi - (i32)i0) + 1u;
-            alive = len >= 32u ? 0xFFFFFFFFu : ((1u << len) - 1u);
-        }
-        if (alive) {
-            ++q.words;
-            const u32 u = i0 + v.OFF;
-            u32 bw[NPP];
-            Planes<NPP>::win(v.P, u, bw);
-            // stages in batches of SB: the batch's window loads are independent and
-            // issue back to back, so their latency is paid once per batch
-            constexpr int SB = NPP == 4 ? CZ_SB4 : (NPP == 2 ? CZ_SB2 : CZ_SB1);
-            u32 j = 1;
-            while (j < t && alive) {
-                u32 m[SB];
-#pragma unroll
-                for (int k = 0; k < SB; ++k)
-                    m[k] = (j + (u32)k < t) ? mismatch<NPP>(v.P, u - (j + (u32)k) * dd, bw) : 0u;
-#pragma unroll
-                for (int k = 0; k < SB; ++k) alive &= ~m[k];
-                j += SB;
-            }
-            q.tests += min(j, t) * (u32)NPP;
-        }
-        const bool has = alive != 0u;
-        const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
-        if (bal) {
-            const u32 pos = __popc(bal & ((1u << lane) - 1u));
-            if (has) sb[q.nscr + pos] = make_uint2(i0, alive);
-            q.nscr += __popc(bal);
-            __syncwarp();
-            if (q.nscr >= 32u)
-                screen_batch<NPP>(c, v, sb, cb, q, 32u, d, dd, t, h, tune.screen != 0u, dinv, have_inv, st, lane);
-        }
-    }
-    if (q.nscr)
-        screen_batch<NPP>(c, v, sb, cb, q, q.nscr, d, dd, t, h, tune.screen != 0u, dinv, have_inv, st, lane);
-}
-
 // queue one 32-bit half-word per lane for the batched screen (the batch runs
 // as soon as 32 are waiting)
 template <int NPP>
-__device__ __forceinline__ void queue_words(const ProfCtx &c, const View &v, uint2 *sb, Cand *cb, WarpQ &q,
-                                            u32 i0, u32 alive, u32 d, u32 dd, u32 t, u32 h, bool screen,
-                                            u32 &dinv, bool &have_inv, ProfState *st, int lane) {
+__device__ __forceinline__ void queue_words(const ProfCtx &c, uint4 *sb, Cand *cb, WarpQ &q, u32 i0, u32 alive,
+                                            u32 d, u32 t, bool screen, ProfState *st, int lane) {
     const bool has = alive != 0u;
     const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
     if (!bal) return;
     const u32 pos = __popc(bal & ((1u << lane) - 1u));
-    if (has) sb[q.nscr + pos] = make_uint2(i0, alive);
+    if (has) sb[q.nscr + pos] = make_uint4(i0, alive, d, t);
     q.nscr += __popc(bal);
     __syncwarp();
-    if (q.nscr >= 32u) screen_batch<NPP>(c, v, sb, cb, q, 32u, d, dd, t, h, screen, dinv, have_inv, st, lane);
+    if (q.nscr >= 32u) screen_batch<NPP>(c, sb, cb, q, 32u, screen, st, lane);
 }
 
 // all selected words of row d on view v, 64 anchors per lane-word: per stage
@@ -428,8 +369,8 @@ __device__ __forceinline__ void queue_words(const ProfCtx &c, const View &v, uin
 // anchors, so ALU work and L1 requests per anchor-stage drop against 32-bit
 // words for a few more stages per word
 template <int NPP>
-__device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref, u32 d, u32 t, u32 s, u32 h,
-                                             const Tuning &tune, uint2 *sb, Cand *cb, WarpQ &q, ProfState *st,
+__device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref, u32 d, u32 t, u32 s,
+                                             const Tuning &tune, uint4 *sb, Cand *cb, WarpQ &q, ProfState *st,
                                              int lane) {
     const View v = vref;
     const u32 G = v.G, dd = d / G;
@@ -442,8 +383,6 @@ __device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref,
     const u32 W = K * nw;
     const float rnw = 1.0f / (float)nw;
     const bool screen = tune.screen != 0u;
-    u32 dinv = 0;
-    bool have_inv = false;
     for (u32 base = 0; base < W; base += 32u) {
         const u32 rank = base + (u32)lane;
         u64 alive = 0;
@@ -478,18 +417,16 @@ __device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref,
             }
             q.tests += 2u * min(j, t) * (u32)NPP;
         }
-        queue_words<NPP>(c, v, sb, cb, q, i0, (u32)alive, d, dd, t, h, screen, dinv, have_inv, st, lane);
-        queue_words<NPP>(c, v, sb, cb, q, i0 + 32u, (u32)(alive >> 32), d, dd, t, h, screen, dinv, have_inv, st,
-                         lane);
+        queue_words<NPP>(c, sb, cb, q, i0, (u32)alive, d, t, screen, st, lane);
+        queue_words<NPP>(c, sb, cb, q, i0 + 32u, (u32)(alive >> 32), d, t, screen, st, lane);
     }
-    if (q.nscr) screen_batch<NPP>(c, v, sb, cb, q, q.nscr, d, dd, t, h, screen, dinv, have_inv, st, lane);
 }
 
 __global__ void __launch_bounds__(SPARSE_WARPS * 32, CZ_SPARSE_MINB)
 sparse_kernel(SparseArgs a) {
-    __shared__ u32 s_item, s_err, s_qspec;
+    __shared__ u32 s_item, s_err;
     __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];      // candidates awaiting completion
-    __shared__ uint2 sbuf[SPARSE_WARPS][CAND_CAP];     // (index, alive) words awaiting the screen
+    __shared__ uint4 sbuf[SPARSE_WARPS][CAND_CAP];     // (index, alive, d, t) words awaiting the screen
     __shared__ ProfCtx s_ctx;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (;;) {
@@ -511,8 +448,9 @@ sparse_kernel(SparseArgs a) {
                 c.odd = View{c.P + (size_t)PR.nwords * PD.npp, 32u * PR.K2, -(i32)((PR.B + 1u) / 2u),
                              (i32)((PR.B - 1u) / 2u), 2u, 1u};
                 for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
+                c.seed = *(volatile u32 *)&a.state[gprof].seed;
+                c.qspec = PD.qspec;
                 s_ctx = c;
-                s_qspec = PD.qspec;
             }
         }
         __syncthreads();
@@ -520,38 +458,33 @@ sparse_kernel(SparseArgs a) {
         if (item >= a.nlist) return;
         const ProfCtx &c = s_ctx;
         ProfState *st = a.state + a.prof_list[item];
-        const u32 seed = *(volatile u32 *)&st->seed;
-        const u32 qspec = s_qspec;
         const u32 tpref = anchor_pref(c.r, a.tune.anchor_bits);
         WarpQ q{0, 0, 0, 0, 0, 0, 0};
-        uint2 *sb = sbuf[warp];
+        uint4 *sb = sbuf[warp];
         Cand *cb = cbuf[warp];
         for (;;) {
             u32 d = 0;
             if (lane == 0) d = atomicAdd(&st->rows_next, 1u) + 1u;     // rows in increasing d
             d = __shfl_sync(0xFFFFFFFFu, d, 0);
             if (d > c.D) break;
-            // row parameters from the verified maximum so far (<= M)
-            const u64 bk = *(volatile unsigned long long *)&st->best;
-            u32 blen = key_len(bk) > seed ? key_len(bk) : seed;
-            // a speculative threshold: every run >= blen is still completed; if the
-            // final best stays below qspec the profile is re-run without it
-            if (qspec > blen) blen = qspec;
+            // row parameters from the verified maximum so far (<= M); with a
+            // speculative threshold every run >= it is still completed, and a
+            // profile whose best stays below it is re-run without it
+            const u32 blen = threshold(c, st);
             const u32 q_ = blen < c.Q ? blen : c.Q;
             if (q_ < 3u) { q.err |= 2u; break; }
             const u32 t = tpref < q_ ? (tpref < 2u ? 2u : tpref) : q_;
             const u32 s = q_ - t + 1u;
-            const u32 h = blen > t ? blen - t : 0u;      // screen: reject runs certified < blen
             const View &v = (d & 1u) ? c.base : c.odd;
-#if CZ_WORD64
-            if (c.npp == 1u) filter_row64<1>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
-            else if (c.npp == 2u) filter_row64<2>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
-            else filter_row64<4>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
-#else
-            if (c.npp == 1u) filter_row<1>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
-            else if (c.npp == 2u) filter_row<2>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
-            else filter_row<4>(c, v, d, t, s, h, a.tune, sb, cb, q, st, lane);
-#endif
+            if (c.npp == 1u) filter_row64<1>(c, v, d, t, s, a.tune, sb, cb, q, st, lane);
+            else if (c.npp == 2u) filter_row64<2>(c, v, d, t, s, a.tune, sb, cb, q, st, lane);
+            else filter_row64<4>(c, v, d, t, s, a.tune, sb, cb, q, st, lane);
+        }
+        // the screen queue carries across rows: drain it, then the candidates
+        if (q.nscr) {
+            if (c.npp == 1u) screen_batch<1>(c, sb, cb, q, q.nscr, a.tune.screen != 0u, st, lane);
+            else if (c.npp == 2u) screen_batch<2>(c, sb, cb, q, q.nscr, a.tune.screen != 0u, st, lane);
+            else screen_batch<4>(c, sb, cb, q, q.nscr, a.tune.screen != 0u, st, lane);
         }
         if (q.ncand) flush_cands(c, cb, q, q.ncand, st, lane);
         if (q.err) atomicOr(&s_err, q.err);

@@ -69,6 +69,7 @@ typedef struct cz_config {
     uint32_t spec_margin10[10];  /* margin per order r, in tenths */
     uint32_t plane_budget_mb;    /* plane pool per wave; larger batches run as consecutive waves */
     uint32_t dense_steps;        /* dense scan segment: 32 x dense_steps values of x per warp */
+    uint32_t anchor_t[10];       /* anchor stages per order r (index r), 2..32; 0: from anchor_bits */
     uint32_t reserved[1];
 } cz_config;
 

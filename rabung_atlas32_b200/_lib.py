@@ -28,7 +28,7 @@ class cz_config(ctypes.Structure):
                 ("anchor_bits", u32), ("screen", u32), ("sparse_blocks", u32), ("use_graph", u32),
                 ("cta_per_profile", u32), ("l1_carveout", u32), ("speculate", u32),
                 ("spec_margin10", u32 * 10), ("plane_budget_mb", u32), ("dense_steps", u32),
-                ("reserved", u32 * 1)]
+                ("anchor_t", u32 * 10), ("reserved", u32 * 1)]
 
 
 class cz_stats(ctypes.Structure):

@@ -4,7 +4,8 @@
 
 Searches, by coordinate descent from the defaults, the knobs that set how the
 work is cut and scheduled:
-  * anchor filter: anchor length policy (anchor_bits), CTAs per profile
+  * anchor filter: anchor length policy (anchor_bits, then stages per order
+    r, anchor_t), CTAs per profile
     (cta_per_profile: warps sharing one profile's row queue), L1 carveout,
     cover shape (cover_n: table radius vs rows), on a sample of the block below
     2^32;
@@ -62,6 +63,15 @@ def _measure(t: Tuning, primes, mode: str, reps: int = 2):
         return best, recs
 
 
+def anchor_pref(r: int, bits: int) -> int:
+    """Stages the filter derives from anchor_bits: least t with r^(t-1) >= 2^(5+bits)."""
+    k, pw = 0, 1
+    while pw < 1 << (5 + bits):
+        pw *= r
+        k += 1
+    return k + 1
+
+
 def tune(quick: bool = False, log=print) -> dict:
     base = Tuning()
     top = sieve.primes_ending(4294967291, 512 if quick else 1024)
@@ -85,6 +95,22 @@ def tune(quick: bool = False, log=print) -> dict:
                 log(f"  {knob}={v}: {ms:.1f} ms")
                 if ms < best_ms * 0.99:
                     best, best_ms = t, ms
+    # anchor stages per order r, one step either side of the current choice
+    for r in range(2, 10):
+        cur = best.anchor_t[r] or anchor_pref(r, best.anchor_bits)
+        for v in (cur - 1, cur + 1):
+            if not 2 <= v <= 32:
+                continue
+            at = list(best.anchor_t)
+            at[r] = v
+            t = dataclasses.replace(best, anchor_t=tuple(at))
+            ms, recs = _measure(t, top, "sparse")
+            if recs != ref:
+                rejected.append({"anchor_t": r, "t": v})
+                continue
+            log(f"  anchor_t[{r}]={v}: {ms:.1f} ms")
+            if ms < best_ms * 0.995:
+                best, best_ms = t, ms
     # dense segment length near 2^22
     mid = sieve.primes_from(1 << 22, 128 if quick else 256)
     dref_ms, dref = _measure(best, mid, "dense")

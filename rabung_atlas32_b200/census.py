@@ -36,6 +36,7 @@ class Tuning:
     spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 15, 15, 15, 15)
     plane_budget_mb: int = 24 * 1024
     dense_steps: int = 256
+    anchor_t: tuple = (0, 0, 11, 7, 6, 5, 4, 4, 4, 4)
 
 
 def _as_u32_array(values):
@@ -86,6 +87,8 @@ class Census:
             cfg.spec_margin10[r] = t.spec_margin10[r]
         cfg.plane_budget_mb = t.plane_budget_mb
         cfg.dense_steps = t.dense_steps
+        for r in range(10):
+            cfg.anchor_t[r] = t.anchor_t[r]
         h = ctypes.c_void_p()
         rc = self.lib.cz_open(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:

@@ -259,6 +259,7 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
                 D.Q = q_for(c, r);
                 D.D = Ds[k];
                 D.qspec = qspec_for(c, p, r, !(flags & CZ_NOSPEC));
+                D.tpref = c.anchor_t[r] ? c.anchor_t[r] : anchor_pref(r, c.anchor_bits);
                 D.plane_off = plane_words;              // multiple of 4 words: vector loads align
                 plane_words += ((u64)D.npp * (P.nwords + P.nwords2) + 3ull) & ~3ull;
                 D.local = (u32)h->h_sidx.size() - 1u;
@@ -399,7 +400,6 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
         sa.nlist = h->nsl;
         sa.next = P<u32>(h->b_counter);
         sa.group = std::max(1u, h->cfg.cta_per_profile);
-        sa.tune.anchor_bits = h->cfg.anchor_bits;
         sa.tune.screen = h->cfg.screen;
         u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : 2u * (u32)h->sms;
         grid = std::min(grid, h->nsl * sa.group);
@@ -505,6 +505,8 @@ int cz_default_config(cz_config *c) {
     c->dense_steps = DENSE_STEPS;
     const u32 sm[10] = {0, 0, 30, 20, 15, 15, 15, 15, 15, 15};
     for (int r = 0; r < 10; ++r) c->spec_margin10[r] = sm[r];
+    const u32 at[10] = {0, 0, 11, 7, 6, 5, 4, 4, 4, 4};   // measured per order on a top block
+    for (int r = 0; r < 10; ++r) c->anchor_t[r] = at[r];
     return CZ_OK;
 }
 
@@ -516,6 +518,8 @@ int cz_open(const cz_config *cfg, cz_handle **out) {
     if (h->cfg.cover_n < 2 || h->cfg.cover_n > 8) { delete h; return CZ_EINVAL; }
     for (int r = 2; r <= 9; ++r)
         if (h->cfg.q_cap[r] && (h->cfg.q_cap[r] < 3 || h->cfg.q_cap[r] > 255)) { delete h; return CZ_EINVAL; }
+    for (int r = 0; r < 10; ++r)
+        if (h->cfg.anchor_t[r] && (h->cfg.anchor_t[r] < 2 || h->cfg.anchor_t[r] > 32)) { delete h; return CZ_EINVAL; }
     h->dev = h->cfg.device;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || h->dev < 0 || h->dev >= ndev) { delete h; return CZ_ECUDA; }

@@ -142,6 +142,7 @@ struct ProfDesc {
     u32 omega[9];    // Montgomery omega^j, omega = z^(m/r), j < r
     u32 local;       // index of the prime within its route's list
     u32 qspec;       // speculative threshold (0: none); exact if the best run reaches it
+    u32 tpref;       // preferred anchor stages (sparse filter)
 };
 
 // device-written per-profile results

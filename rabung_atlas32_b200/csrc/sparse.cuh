@@ -62,7 +62,6 @@ constexpr int CAND_CAP = 64;          // per-warp buffers
 constexpr u32 RUN_CAP = 4096;         // longest run a completion may walk
 
 struct Tuning {
-    u32 anchor_bits;   // t chosen so 32 * r^-(t-1) <= 2^-anchor_bits per word
     u32 screen;        // 1: bilateral screen on
 };
 
@@ -82,7 +81,7 @@ struct Cand { u32 b, d; };
 
 // preferred anchor length: least t with r^(t-1) >= 2^(5+bits), i.e. a word of
 // 32 random anchors keeps on average <= 2^-bits survivors
-__device__ __forceinline__ u32 anchor_pref(u32 r, u32 bits) {
+CZ_HD u32 anchor_pref(u32 r, u32 bits) {
     const u64 goal = u64(1) << (5u + bits);
     u64 pw = 1;
     u32 k = 0;
@@ -178,6 +177,7 @@ struct ProfCtx {
     View base, odd;
     u32 om[9];
     u32 seed, qspec;       // certified stretch from the table, speculative threshold
+    u32 tpref;             // preferred anchor stages for this order
 };
 
 // colour of numerator n (|n| <= B) as an integer, from the base view
@@ -450,6 +450,7 @@ sparse_kernel(SparseArgs a) {
                 for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
                 c.seed = *(volatile u32 *)&a.state[gprof].seed;
                 c.qspec = PD.qspec;
+                c.tpref = PD.tpref;
                 s_ctx = c;
             }
         }
@@ -458,7 +459,7 @@ sparse_kernel(SparseArgs a) {
         if (item >= a.nlist) return;
         const ProfCtx &c = s_ctx;
         ProfState *st = a.state + a.prof_list[item];
-        const u32 tpref = anchor_pref(c.r, a.tune.anchor_bits);
+        const u32 tpref = c.tpref;
         WarpQ q{0, 0, 0, 0, 0, 0, 0};
         uint4 *sb = sbuf[warp];
         Cand *cb = cbuf[warp];

@@ -26,7 +26,7 @@ def test_header_symbols_exported():
 def test_struct_layouts():
     from rabung_atlas32_b200 import _lib
     assert ctypes.sizeof(_lib.cz_profile) == 32
-    assert ctypes.sizeof(_lib.cz_config) == 4 * (1 + 1 + 1 + 10 + 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 1)
+    assert ctypes.sizeof(_lib.cz_config) == 4 * (1 + 1 + 1 + 10 + 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 10 + 1)
 
 
 def test_count_profiles_host_only():
@@ -35,3 +35,24 @@ def test_count_profiles_host_only():
     ps = [2, 3, 5, 7, 4294967291]
     arr = (ctypes.c_uint32 * len(ps))(*ps)
     assert lib.cz_count_profiles(arr, len(ps)) == sum(bin(codec.expected_mask(p)).count("1") for p in ps[1:])
+
+
+def test_default_config_and_bad_tuning_refused_before_device():
+    """cz_default_config fills the measured per-order anchor stages; cz_open
+    validates a tuning before it looks for a device, so a bad one is refused
+    with CZ_EINVAL on any host."""
+    from rabung_atlas32_b200 import _lib
+    from rabung_atlas32_b200.census import Tuning
+    lib = _lib.load()
+    cfg = _lib.cz_config()
+    assert lib.cz_default_config(ctypes.byref(cfg)) == _lib.CZ_OK
+    assert tuple(cfg.anchor_t) == Tuning().anchor_t
+    assert tuple(cfg.q_cap) == Tuning().q_cap and tuple(cfg.spec_margin10) == Tuning().spec_margin10
+    h = ctypes.c_void_p()
+    for field, r, bad in [("anchor_t", 5, 1), ("anchor_t", 2, 33), ("q_cap", 3, 2), ("q_cap", 9, 256)]:
+        lib.cz_default_config(ctypes.byref(cfg))
+        getattr(cfg, field)[r] = bad
+        assert lib.cz_open(ctypes.byref(cfg), ctypes.byref(h)) == _lib.CZ_EINVAL, (field, r, bad)
+    lib.cz_default_config(ctypes.byref(cfg))
+    cfg.cover_n = 1
+    assert lib.cz_open(ctypes.byref(cfg), ctypes.byref(h)) == _lib.CZ_EINVAL

@@ -160,6 +160,19 @@ def test_replay_bit_identical(eng):
     assert tup(a) == tup(b)
 
 
+def test_anchor_stages_do_not_change_records():
+    """The per-order anchor stage counts trade filter work for screen and
+    completion work; the records are certified either way and must not move."""
+    import dataclasses
+    from rabung_atlas32_b200.census import Census, Tuning
+    ps = sieve.primes_ending(4294967291, 64)
+    with Census(tuning=Tuning()) as c0:
+        want = tup(c0.profiles(ps, mode="sparse", a4=False))
+    for at in [(0, 0, 2, 2, 2, 2, 2, 2, 2, 2), (0, 0, 16, 10, 9, 8, 7, 7, 6, 6), (0,) * 10]:
+        with Census(tuning=dataclasses.replace(Tuning(), anchor_t=at)) as c1:
+            assert tup(c1.profiles(ps, mode="sparse", a4=False)) == want, at
+
+
 def test_speculation_miss_rerun_exact():
     """Speculative thresholds at floor(log_r p) (margin 0) miss often; every miss
     is re-run without speculation and the records equal the unspeculated ones."""

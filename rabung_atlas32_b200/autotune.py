@@ -5,7 +5,7 @@
 Searches, by coordinate descent from the defaults, the knobs that set how the
 work is cut and scheduled:
   * anchor filter: anchor length policy (anchor_bits, then stages per order
-    r, anchor_t), CTAs per profile
+    r, anchor_t), speculation margin per order r, CTAs per profile
     (cta_per_profile: warps sharing one profile's row queue), L1 carveout,
     cover shape (cover_n: table radius vs rows), on a sample of the block below
     2^32;
@@ -109,6 +109,23 @@ def tune(quick: bool = False, log=print) -> dict:
                 rejected.append({"anchor_t": r, "t": v})
                 continue
             log(f"  anchor_t[{r}]={v}: {ms:.1f} ms")
+            if ms < best_ms * 0.995:
+                best, best_ms = t, ms
+    # speculation margin per order r (tenths); the measured time includes the
+    # re-runs of the primes whose best run stayed below the threshold
+    for r in range(2, 10):
+        cur = best.spec_margin10[r]
+        for v in (cur - 10, cur - 5, cur + 5, cur + 10):
+            if not 0 <= v <= 60:
+                continue
+            sm = list(best.spec_margin10)
+            sm[r] = v
+            t = dataclasses.replace(best, spec_margin10=tuple(sm))
+            ms, recs = _measure(t, top, "sparse")
+            if recs != ref:
+                rejected.append({"spec_margin10": r, "margin": v})
+                continue
+            log(f"  spec_margin10[{r}]={v}: {ms:.1f} ms")
             if ms < best_ms * 0.995:
                 best, best_ms = t, ms
     # dense segment length near 2^22

@@ -33,7 +33,7 @@ class Tuning:
     cta_per_profile: int = 2
     l1_carveout: int = 20
     speculate: int = 1
-    spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 15, 15, 15, 15)
+    spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 10, 0, 5, 10)
     plane_budget_mb: int = 24 * 1024
     dense_steps: int = 256
     anchor_t: tuple = (0, 0, 11, 7, 6, 5, 4, 4, 4, 4)

@@ -5,7 +5,7 @@
 Searches, by coordinate descent from the defaults, the knobs that set how the
 work is cut and scheduled:
   * anchor filter: anchor length policy (anchor_bits, then stages per order
-    r, anchor_t), speculation margin per order r, CTAs per profile
+    r, anchor_t), cover window cap and speculation margin per order r, CTAs per profile
     (cta_per_profile: warps sharing one profile's row queue), L1 carveout,
     cover shape (cover_n: table radius vs rows), on a sample of the block below
     2^32;
@@ -109,6 +109,23 @@ def tune(quick: bool = False, log=print) -> dict:
                 rejected.append({"anchor_t": r, "t": v})
                 continue
             log(f"  anchor_t[{r}]={v}: {ms:.1f} ms")
+            if ms < best_ms * 0.995:
+                best, best_ms = t, ms
+    # cover window cap per order r: q never exceeds it, and the largest cap of
+    # a prime's orders sets its table radius
+    for r in range(2, 10):
+        cur = best.q_cap[r]
+        for v in (cur - 4, cur - 2, cur + 2):
+            if not 3 <= v <= 255:
+                continue
+            qc = list(best.q_cap)
+            qc[r] = v
+            t = dataclasses.replace(best, q_cap=tuple(qc))
+            ms, recs = _measure(t, top, "sparse")
+            if recs != ref:
+                rejected.append({"q_cap": r, "Q": v})
+                continue
+            log(f"  q_cap[{r}]={v}: {ms:.1f} ms")
             if ms < best_ms * 0.995:
                 best, best_ms = t, ms
     # speculation margin per order r (tenths); the measured time includes the

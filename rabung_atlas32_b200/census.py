@@ -25,7 +25,7 @@ class CensusError(RuntimeError):
 class Tuning:
     sparse_min_p: int = 1 << 20
     cover_n: int = 3
-    q_cap: tuple = (0, 0, 40, 24, 20, 16, 16, 15, 14, 13)
+    q_cap: tuple = (0, 0, 30, 24, 20, 16, 16, 15, 14, 13)
     anchor_bits: int = 4
     screen: int = 1
     sparse_blocks: int = 0

@@ -492,7 +492,7 @@ int cz_default_config(cz_config *c) {
     c->device = 0;
     c->sparse_min_p = 1u << 20;
     c->cover_n = 3;
-    const u32 q[10] = {0, 0, 40, 24, 20, 16, 16, 15, 14, 13};
+    const u32 q[10] = {0, 0, 30, 24, 20, 16, 16, 15, 14, 13};
     for (int r = 0; r < 10; ++r) c->q_cap[r] = q[r];
     c->anchor_bits = 4;
     c->screen = 1;

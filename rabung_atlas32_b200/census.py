@@ -209,3 +209,32 @@ class Census:
             primes = primes_in(lo, hi)
         recs = self.profiles(primes, mode=mode, a4=True)
         return codec.encode_scan_frame(lo, hi, recs), codec.encode_a4_frame(lo, hi, recs), recs
+
+
+def main(argv=None):
+    """One census of a window of consecutive primes, printing the call's stats:
+
+        python -m rabung_atlas32_b200.census --ending 4294967291 --count 512 --mode sparse
+        python -m rabung_atlas32_b200.census --from 16777216 --count 4096 --mode dense --a4
+    """
+    import argparse
+    import json
+    from . import sieve
+    ap = argparse.ArgumentParser(description=main.__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    g = ap.add_mutually_exclusive_group(required=True)
+    g.add_argument("--ending", type=int, help="the window ends at this prime")
+    g.add_argument("--from", dest="start", type=int, help="the window starts at the first prime >= this")
+    ap.add_argument("--count", type=int, default=4096)
+    ap.add_argument("--mode", default="auto", choices=list(MODES))
+    ap.add_argument("--a4", action="store_true")
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args(argv)
+    ps = sieve.primes_ending(a.ending, a.count) if a.ending else sieve.primes_from(a.start, a.count)
+    with Census() as c:
+        for _ in range(a.repeat):
+            _, _, st = c.raw(ps, mode=a.mode, a4=a.a4)
+            print(json.dumps({k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()}))
+
+
+if __name__ == "__main__":
+    main()

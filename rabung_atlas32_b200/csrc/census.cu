@@ -260,8 +260,8 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
                 D.D = Ds[k];
                 D.qspec = qspec_for(c, p, r, !(flags & CZ_NOSPEC));
                 D.tpref = c.anchor_t[r] ? c.anchor_t[r] : anchor_pref(r, c.anchor_bits);
-                D.plane_off = plane_words;              // multiple of 4 words: vector loads align
-                plane_words += ((u64)D.npp * (P.nwords + P.nwords2) + 3ull) & ~3ull;
+                D.plane_off = plane_words;              // multiple of 8 words: 256-bit loads align
+                plane_words += ((u64)D.npp * (P.nwords + P.nwords2) + 7ull) & ~7ull;
                 D.local = (u32)h->h_sidx.size() - 1u;
                 h->h_slist.push_back((u32)h->hprof.size());
             } else {

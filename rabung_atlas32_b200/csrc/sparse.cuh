@@ -89,6 +89,13 @@ CZ_HD u32 anchor_pref(u32 r, u32 bits) {
     return k + 1u;
 }
 
+// 256-bit read-only load (sm_100), 32-byte aligned address
+__device__ __forceinline__ void ld_nc_256(const u32 *p, uint4 &lo, uint4 &hi) {
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(lo.x), "=r"(lo.y), "=r"(lo.z), "=r"(lo.w), "=r"(hi.x), "=r"(hi.y), "=r"(hi.z), "=r"(hi.w)
+        : "l"(p));
+}
+
 // windows of all NPP interleaved planes at bit index u
 template <int NPP> struct Planes;
 template <> struct Planes<1> {
@@ -129,9 +136,17 @@ template <> struct Planes<4> {
         o[2] = __funnelshift_r(a.z, b.z, sh);
         o[3] = __funnelshift_r(a.w, b.w, sh);
     }
+    // the three plane groups of a 64-bit window from two aligned 256-bit
+    // loads (view bases are 32-byte aligned; the fourth group read lies in
+    // the view's padding)
     static __device__ __forceinline__ void win64(const u32 *__restrict__ P, u32 u, u32 *lo, u32 *hi) {
-        const uint4 *q = reinterpret_cast<const uint4 *>(P) + (u >> 5);
-        const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+        const u32 wi = u >> 5;
+        const u32 *q = P + 8u * (wi >> 1);
+        uint4 x0, x1, y0, y1;
+        ld_nc_256(q, x0, x1);
+        ld_nc_256(q + 8, y0, y1);
+        const bool odd = wi & 1u;
+        const uint4 a = odd ? x1 : x0, b = odd ? y0 : x1, c = odd ? y1 : y0;
         const u32 sh = u & 31u;
         lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
         lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);

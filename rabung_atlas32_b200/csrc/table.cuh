@@ -54,6 +54,7 @@ struct TableArgs {
 
 struct TabProf {            // per-profile constants of the CTA's prime
     u32 r, magic, npp, sig;
+    u32 seed;               // 1: track the seed stretch (no speculative threshold)
     u32 *base, *odd;
 };
 
@@ -102,6 +103,12 @@ table_kernel(TableArgs a) {
             t.magic = magic_of(D.r);
             t.npp = D.npp;
             t.sig = mod_small(P.sigma, D.r, t.magic);
+            // a profile with a speculative threshold is certified by its best
+            // run reaching q_spec (else it is re-run unspeculated, seed and
+            // all), so its records never depend on the seed; the seed would
+            // only raise its starting threshold when a stretch inside [1, B]
+            // beat q_spec, which the margins make rare
+            t.seed = D.qspec == 0u ? 1u : 0u;
             t.base = a.planes + D.plane_off;
             t.odd = a.planes + D.plane_off + (u64)P.nwords * D.npp;
             tp[threadIdx.x] = t;
@@ -223,7 +230,7 @@ table_kernel(TableArgs a) {
                     }
                     // longest monochromatic stretch inside [1, B] (n = 1 starts a run)
                     const bool sv = n >= 1u && n <= B;
-                    const u32 V = __ballot_sync(0xFFFFFFFFu, sv);
+                    const u32 V = t.seed ? __ballot_sync(0xFFFFFFFFu, sv) : 0u;
                     if (V) {
                         const u32 fv = (u32)(__ffs(V) - 1), top = 31u - __clz(V);
                         u32 pc = __shfl_up_sync(0xFFFFFFFFu, c, 1);

@@ -277,6 +277,14 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
     h->ndense = (u32)h->h_didx.size();
     h->nsparse = (u32)h->h_sidx.size();
     h->nchunks = h->h_chunk.back();
+    // longest first: the persistent filter hands out profiles in list order,
+    // so the costly ones (more stored planes, larger p) start first and the
+    // launch ends on short profiles
+    std::stable_sort(h->h_slist.begin(), h->h_slist.end(), [h](u32 x, u32 y) {
+        const ProfDesc &a = h->hprof[x], &b = h->hprof[y];
+        if (a.npp != b.npp) return a.npp > b.npp;
+        return h->hp[a.prime].p > h->hp[b.prime].p;
+    });
     h->nsl = (u32)h->h_slist.size();
     h->ndl = (u32)h->h_dlist.size();
     // primes below the largest table end, for the table kernel's shared memory

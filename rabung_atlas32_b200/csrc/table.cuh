@@ -197,6 +197,9 @@ table_kernel(TableArgs a) {
                     const u32 co = __shfl_sync(0xFFFFFFFFu, c, 2 * (lane & 15) + 1);
                     const u32 cno = __shfl_sync(0xFFFFFFFFu, cn, 2 * (lane & 15) + 1);
                     const bool odd_step = (k & 1u) != 0u;
+                    // lane b collects plane b's words; one store per word kind
+                    // then writes the interleaved planes of a word together
+                    u32 vneg = 0u, vpos = 0u, vop = 0u, von = 0u;
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
                         if (b >= (int)t.npp) break;
@@ -205,16 +208,22 @@ table_kernel(TableArgs a) {
                         const u32 hp = __ballot_sync(0xFFFFFFFFu, (co >> b) & 1u) & 0xFFFFu;
                         const u32 hn = __ballot_sync(0xFFFFFFFFu, (cno >> b) & 1u) & 0xFFFFu;
                         if (lane == b) {
-                            t.base[(size_t)(K0 - k) * t.npp + b] = __brev(wn);
-                            if (k >= 1u) t.base[(size_t)(K0 + k) * t.npp + b] = (prevw[b] >> 1) | ((wp & 1u) << 31);
-                            if (odd_step) {
-                                const u32 kap = k >> 1;
-                                t.odd[(size_t)(K2 + kap) * t.npp + b] = stp[b] | (hp << 16);
-                                t.odd[(size_t)(K2 - kap - 1u) * t.npp + b] = __brev(stn[b] | (hn << 16));
-                            }
+                            vneg = __brev(wn);
+                            vpos = (prevw[b] >> 1) | ((wp & 1u) << 31);
+                            vop = stp[b] | (hp << 16);
+                            von = __brev(stn[b] | (hn << 16));
                         }
                         prevw[b] = wp;
                         if (!odd_step) { stp[b] = hp; stn[b] = hn; }
+                    }
+                    if ((u32)lane < t.npp) {
+                        t.base[(size_t)(K0 - k) * t.npp + lane] = vneg;
+                        if (k >= 1u) t.base[(size_t)(K0 + k) * t.npp + lane] = vpos;
+                        if (odd_step) {
+                            const u32 kap = k >> 1;
+                            t.odd[(size_t)(K2 + kap) * t.npp + lane] = vop;
+                            t.odd[(size_t)(K2 - kap - 1u) * t.npp + lane] = von;
+                        }
                     }
                     // odd-view word of a final unpaired even step
                     if (!odd_step && k + 1u == KS) {

@@ -41,7 +41,8 @@ extern "C" {
 #define CZ_EINVAL 1   /* bad argument (not prime, out of domain, buffer too small) */
 #define CZ_ECUDA 2    /* CUDA error */
 #define CZ_EREFUSED 3 /* a device status check failed: the whole request is refused */
-#define CZ_ELIMIT 4   /* request exceeds the fixed limits of cz_census_dense_noalloc */
+#define CZ_ELIMIT 4   /* request exceeds a fixed limit or a caller buffer (nothing written) */
+#define CZ_EPENDING 5 /* cz_poll / cz_next_done: the request is not complete yet */
 
 /* One (p, r) profile, 32 bytes.  Records come grouped by prime in input
  * order and, within a prime, by ascending r. */
@@ -158,6 +159,51 @@ int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_profile *out,
  * profile of one prime for the orders in `mask` (bit r-2), M into out[r] and
  * L into prefix[r] (arrays of >= 10).  Returns 0, or 2 when mask asks for an
  * order that does not divide p-1.  Not thread-safe (one global handle). */
+/* Census of every prime in [lo, hi) (hi <= 2^32): the primes are found by the
+ * device sieve, then censused as by cz_census.  primes_out (capacity
+ * primes_cap) receives them ascending and *n_primes their count; out
+ * (capacity out_cap) the records and *n_profiles their count; a4_out (NULL, or
+ * capacity primes_cap) A4 per prime when flags has CZ_A4.  When a capacity is
+ * too small the call returns CZ_ELIMIT with the needed counts in *n_primes /
+ * *n_profiles (n_profiles 0 if the primes did not fit) and no records.  One
+ * call replaces a supervisor's sieve of a block plus the worker round trip
+ * (src/census/prime_sieve.cpp:8-22, src/census/worker32.cu:10-45). */
+int cz_census_interval(cz_handle *h, uint64_t lo, uint64_t hi, uint32_t flags, uint32_t *primes_out,
+                       uint32_t primes_cap, uint32_t *n_primes, cz_profile *out, uint32_t out_cap,
+                       uint32_t *n_profiles, uint32_t *a4_out, cz_stats *stats);
+
+/* ---- serving ---------------------------------------------------------------
+ * A server owns `slots` handles (one CUDA stream each) and one worker thread
+ * per slot.  Requests wait in arrival order; whenever a slot is free it admits
+ * every waiting request (same flags) whose colour-plane pool still fits the
+ * slot budget and the GPU's free memory, sieves the batch's intervals on the
+ * device, censuses the batch in one merged call and holds each request's
+ * records until they are polled.  A merged call that is refused is re-run
+ * request by request, so a refusal reaches only the request that caused it.
+ * Submit and poll may be called from any host thread.  The reference has no
+ * serving path; the records equal cz_census's for the same primes. */
+typedef struct cz_server cz_server;
+int cz_server_open(const cz_config *cfg, uint32_t slots, uint64_t slot_budget_bytes, cz_server **out);
+void cz_server_close(cz_server *s);             /* finishes running batches; drops unpolled work */
+/* a request for the `count` consecutive primes from lo (device sieve), or,
+ * when primes != NULL, for those `count` primes; flags as for cz_census */
+int cz_submit(cz_server *s, uint32_t lo, uint32_t count, const uint32_t *primes, uint32_t flags,
+              uint64_t *request_id);
+/* the id of a completed request not yet announced; waits up to timeout_ms
+ * (negative: until one completes); CZ_EPENDING on timeout */
+int cz_next_done(cz_server *s, int32_t timeout_ms, uint64_t *request_id);
+/* waits up to timeout_ms for request_id (CZ_EPENDING if still running); then
+ * copies its primes (capacity primes_cap), records (capacity out_cap) and A4
+ * (capacity primes_cap; any output may be NULL), releases the request and
+ * returns its status (CZ_OK, or the refusal; cz_server_last_error says why).
+ * CZ_ELIMIT with the needed counts when a capacity is too small (the request
+ * is kept). */
+int cz_poll(cz_server *s, uint64_t request_id, int32_t timeout_ms, uint32_t *primes_out, uint32_t primes_cap,
+            uint32_t *n_primes, cz_profile *out, uint32_t out_cap, uint32_t *n_profiles, uint32_t *a4_out);
+/* batches run, requests completed, requests waiting */
+int cz_server_info(cz_server *s, uint64_t *batches, uint64_t *completed, uint64_t *waiting);
+const char *cz_server_last_error(cz_server *s);
+
 void baseline_init(unsigned cap);
 int baseline_profile(unsigned p, unsigned mask, unsigned *out, unsigned *prefix, int full);
 

@@ -13,7 +13,7 @@ from pathlib import Path
 from .build import LIB
 
 CZ_DENSE, CZ_SPARSE, CZ_AUTO, CZ_A4, CZ_VERIFY = 1, 2, 3, 4, 8
-CZ_OK, CZ_EINVAL, CZ_ECUDA, CZ_EREFUSED, CZ_ELIMIT = 0, 1, 2, 3, 4
+CZ_OK, CZ_EINVAL, CZ_ECUDA, CZ_EREFUSED, CZ_ELIMIT, CZ_EPENDING = 0, 1, 2, 3, 4, 5
 
 u32, u64, i32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
 
@@ -46,8 +46,9 @@ class cz_stats(ctypes.Structure):
 
 EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_count_profiles",
            "cz_census", "cz_replay", "cz_a4", "cz_sieve", "cz_plane_bytes", "cz_mem_info", "cz_device_info",
-           "cz_microbench", "cz_census_dense_noalloc", "baseline_init",
-           "baseline_profile"]
+           "cz_microbench", "cz_census_dense_noalloc", "cz_census_interval", "cz_server_open",
+           "cz_server_close", "cz_submit", "cz_next_done", "cz_poll", "cz_server_info", "cz_server_last_error",
+           "baseline_init", "baseline_profile"]
 
 _lib = None
 
@@ -93,6 +94,24 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.cz_census_dense_noalloc.argtypes = [ctypes.POINTER(u32), u32, ctypes.POINTER(cz_profile), u32,
                                           ctypes.c_void_p]
     L.cz_census_dense_noalloc.restype = ctypes.c_int
+    P32, P64 = ctypes.POINTER(u32), ctypes.POINTER(u64)
+    L.cz_census_interval.argtypes = [H, u64, u64, u32, P32, u32, P32, ctypes.POINTER(cz_profile), u32, P32, P32,
+                                     ctypes.POINTER(cz_stats)]
+    L.cz_census_interval.restype = ctypes.c_int
+    L.cz_server_open.argtypes = [ctypes.POINTER(cz_config), u32, u64, ctypes.POINTER(H)]
+    L.cz_server_open.restype = ctypes.c_int
+    L.cz_server_close.argtypes = [H]
+    L.cz_server_close.restype = None
+    L.cz_submit.argtypes = [H, u32, u32, P32, u32, P64]
+    L.cz_submit.restype = ctypes.c_int
+    L.cz_next_done.argtypes = [H, i32, P64]
+    L.cz_next_done.restype = ctypes.c_int
+    L.cz_poll.argtypes = [H, u64, i32, P32, u32, P32, ctypes.POINTER(cz_profile), u32, P32, P32]
+    L.cz_poll.restype = ctypes.c_int
+    L.cz_server_info.argtypes = [H, P64, P64, P64]
+    L.cz_server_info.restype = ctypes.c_int
+    L.cz_server_last_error.argtypes = [H]
+    L.cz_server_last_error.restype = ctypes.c_char_p
     L.baseline_init.argtypes = [ctypes.c_uint]
     L.baseline_init.restype = None
     L.baseline_profile.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),

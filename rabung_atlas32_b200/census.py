@@ -48,6 +48,19 @@ def _as_u32_array(values):
     return arr
 
 
+def to_records(primes, out, a4v) -> list:
+    """codec.Record list from C records grouped by prime in input order."""
+    recs, k = [], 0
+    for i, p in enumerate(primes):
+        rec = codec.Record(int(p), [], a4v[i] if a4v else 0)
+        for _ in range(bin(codec.expected_mask(p)).count("1") if p > 2 else 0):
+            v = out[k]
+            k += 1
+            rec.profiles.append(codec.Profile(v.r, v.M, v.L, v.witness, v.K))
+        recs.append(rec)
+    return recs
+
+
 class Census:
     def __init__(self, device: int = 0, tuning: Tuning | None = None, autoload: bool = True):
         """Open a handle on `device`.  Without an explicit tuning, the
@@ -139,15 +152,25 @@ class Census:
     def profiles(self, primes, mode: str = "auto", a4: bool = True, verify: bool = False):
         """List of codec.Record (profiles ascending r, A4 when requested)."""
         out, a4v, _ = self.raw(primes, mode, a4, verify)
-        recs, k = [], 0
-        for i, p in enumerate(primes):
-            rec = codec.Record(int(p), [], a4v[i] if a4v else 0)
-            for _ in range(bin(codec.expected_mask(p)).count("1") if p > 2 else 0):
-                v = out[k]
-                k += 1
-                rec.profiles.append(codec.Profile(v.r, v.M, v.L, v.witness, v.K))
-            recs.append(rec)
-        return recs
+        return to_records(primes, out, a4v)
+
+    def interval(self, lo: int, hi: int, mode: str = "auto", a4: bool = True, max_primes: int = 1 << 20):
+        """(primes, records) of every prime in [lo, hi): device sieve + census
+        in one library call (cz_census_interval)."""
+        cap = max(1, min(int(max_primes), 1 << 24))
+        ps = (ctypes.c_uint32 * cap)()
+        npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
+        out = (_lib.cz_profile * (8 * cap))()
+        a4buf = (ctypes.c_uint32 * cap)() if a4 else None
+        flags = MODES[mode] | (_lib.CZ_A4 if a4 else 0)
+        st = _lib.cz_stats()
+        rc = self.lib.cz_census_interval(self.h, int(lo), int(hi), flags, ps, cap, ctypes.byref(npr), out, 8 * cap,
+                                         ctypes.byref(nprof), a4buf, ctypes.byref(st))
+        if rc != 0:
+            raise CensusError(f"interval census refused (rc={rc}, primes {npr.value}): {self._err()}")
+        self.last_stats = st.as_dict()
+        primes = list(ps[:npr.value])
+        return primes, to_records(primes, out, list(a4buf[:npr.value]) if a4 else None)
 
     def replay(self) -> dict:
         """Re-run the device work of the last call on its resident inputs."""

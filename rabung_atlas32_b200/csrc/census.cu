@@ -450,6 +450,9 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
     }
     rec(5);
     if ((h->flags & CZ_A4) && h->n) {
+        // the A4 error word is cleared by every call that counts points, also
+        // when no sparse profile cleared the counter block above
+        cudaMemsetAsync(P<u32>(h->b_counter) + 8, 0, 4, st);
         a4_kernel<<<(h->n + A4_WARPS - 1) / A4_WARPS, A4_WARPS * 32, 0, st>>>(P<PrimeDesc>(h->b_primes), h->n,
                                                                            P<u32>(h->b_a4), P<u32>(h->b_counter) + 8);
         ++launches;
@@ -1113,3 +1116,5 @@ int baseline_profile(unsigned p, unsigned mask, unsigned *out, unsigned *prefix,
 }
 
 }  // extern "C"
+
+#include "runtime.cuh"

@@ -1,9 +1,11 @@
 """Serving loop: census requests for prime intervals arriving over time.
 
 A request asks for the profiles (and A4) of the `count` consecutive primes
-starting at `lo`.  The server keeps every request's state resident until it
-completes and runs continuous batching over `slots` in-flight batches (one
-library handle, hence one CUDA stream, per slot):
+starting at `lo`.  `Server` drives the library's native serving runtime
+(cz_server_open / cz_submit / cz_next_done / cz_poll, csrc/runtime.cuh), which
+keeps every request's state resident until it is polled and runs continuous
+batching over `slots` in-flight batches (one library handle, hence one CUDA
+stream and one worker thread, per slot):
 
   * whenever a slot is free, every waiting request that fits is admitted into
     one batch -- admission by device memory: the batch's colour-plane pool must
@@ -24,15 +26,13 @@ reports p50/p99 latency and profiles/s, next to plain per-request calls.
 """
 from __future__ import annotations
 
-import math
-import queue
 import threading
 import time
 from dataclasses import dataclass, field
 
 import numpy as np
 
-from .census import Census, Tuning
+from .census import Census, CensusError, Tuning, to_records
 
 
 @dataclass
@@ -59,102 +59,111 @@ def make_trace(n: int, rate: float, seed: int = 20261203) -> list:
 
 
 class Server:
+    """Continuous batching server: the library's native serving runtime
+    (cz_server_open / cz_submit / cz_next_done / cz_poll) with `slots` slots,
+    each with its own handle and CUDA stream and a slot budget for the colour-
+    plane pools of one batch."""
+
     def __init__(self, slots: int = 2, slot_budget_mb: int = 16 * 1024, device: int = 0,
-                 reserve_mb: int = 4096, max_batch_requests: int = 4096, tuning: Tuning | None = None):
-        self.slots = [Census(device=device, tuning=tuning) for _ in range(slots)]
-        self.slot_budget = slot_budget_mb << 20
-        self.reserve = reserve_mb << 20
-        self.max_batch = max_batch_requests
-        self.waiting: list = []
-        self.cv = threading.Condition()
-        self.closed = False
+                 tuning: Tuning | None = None):
+        import ctypes
+        from . import _lib
+        self._ct, self._L = ctypes, _lib
+        self.lib = _lib.load()
+        probe = Census(device=device, tuning=tuning)      # resolves the tuning saved for this device
+        try:
+            t = probe.tuning
+            cfg = _lib.cz_config()
+            self.lib.cz_default_config(ctypes.byref(cfg))
+            cfg.device = device
+            cfg.sparse_min_p, cfg.cover_n, cfg.anchor_bits, cfg.screen = t.sparse_min_p, t.cover_n, t.anchor_bits, t.screen
+            cfg.sparse_blocks, cfg.use_graph, cfg.cta_per_profile = t.sparse_blocks, t.use_graph, t.cta_per_profile
+            cfg.l1_carveout, cfg.speculate, cfg.plane_budget_mb = t.l1_carveout, t.speculate, t.plane_budget_mb
+            cfg.dense_steps = t.dense_steps
+            for r in range(10):
+                cfg.q_cap[r], cfg.spec_margin10[r], cfg.anchor_t[r] = t.q_cap[r], t.spec_margin10[r], t.anchor_t[r]
+        finally:
+            probe.close()
+        h = ctypes.c_void_p()
+        rc = self.lib.cz_server_open(ctypes.byref(cfg), slots, slot_budget_mb << 20, ctypes.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"cz_server_open failed (rc={rc})")
+        self.h = h
         self.t0 = 0.0
-        self.batches = 0
-        self.error: Exception | None = None
+
+    @property
+    def batches(self) -> int:
+        b = self._ct.c_uint64()
+        self.lib.cz_server_info(self.h, self._ct.byref(b), None, None)
+        return int(b.value)
 
     def close(self):
-        for s in self.slots:
-            s.close()
+        if self.h is not None:
+            self.lib.cz_server_close(self.h)
+            self.h = None
 
-    # -- admission ------------------------------------------------------------
-    def _admit(self, eng: Census) -> list:
-        """Take waiting requests (arrival order) while the batch fits memory."""
-        free, _ = eng.mem_info()
-        cap = min(self.slot_budget, max(0, free - self.reserve))
-        batch, used = [], 0
-        keep = []
-        for r in self.waiting:
-            if len(batch) >= self.max_batch:
-                keep.append(r)
-                continue
-            # upper estimate of the request's planes: its count primes near lo's top
-            est = eng.plane_bytes([min(2 ** 32 - 5, int(r.lo + r.count * max(1.0, math.log(r.lo + 2)) * 1.3))])
-            est *= r.count
-            if batch and used + est > cap:
-                keep.append(r)
-                continue
-            batch.append(r)
-            used += est
-        self.waiting = keep
-        return batch
+    def submit(self, lo: int, count: int, flags: int | None = None) -> int:
+        ct = self._ct
+        rid = ct.c_uint64()
+        fl = (self._L.CZ_AUTO | self._L.CZ_A4) if flags is None else flags
+        rc = self.lib.cz_submit(self.h, int(lo), int(count), None, fl, ct.byref(rid))
+        if rc != 0:
+            raise RuntimeError(f"cz_submit failed (rc={rc})")
+        return int(rid.value)
 
-    # -- one slot -------------------------------------------------------------
-    def _slot_loop(self, k: int):
-        eng = self.slots[k]
-        while True:
-            with self.cv:
-                while not self.waiting and not self.closed:
-                    self.cv.wait()
-                if not self.waiting and self.closed:
-                    return
-                batch = self._admit(eng)
-                self.batches += 1
-                bid = self.batches
-            try:
-                self._run_batch(eng, batch, bid)
-            except Exception as e:          # a refused batch fails the whole run
-                self.error = e
-                with self.cv:
-                    self.closed = True
-                    self.cv.notify_all()
-                return
+    def next_done(self, timeout_ms: int) -> int | None:
+        rid = self._ct.c_uint64()
+        rc = self.lib.cz_next_done(self.h, int(timeout_ms), self._ct.byref(rid))
+        return int(rid.value) if rc == self._L.CZ_OK else None
 
-    def _run_batch(self, eng: Census, batch: list, bid: int):
-        primes_per = eng.sieve([(r.lo, r.count) for r in batch])      # device sieve
-        flat = [p for ps in primes_per for p in ps]
-        recs = eng.profiles(flat, mode="auto", a4=True) if flat else []
-        k = 0
-        now = time.perf_counter() - self.t0
-        for r, ps in zip(batch, primes_per):
-            r.primes = ps
-            r.records = recs[k:k + len(ps)]
-            k += len(ps)
-            r.done = now
-            r.batch = bid
+    def fetch(self, rid: int, count: int) -> tuple:
+        """(primes, records) of a completed request (releases it)."""
+        ct, L = self._ct, self._L
+        ps = (ct.c_uint32 * max(1, count))()
+        out = (L.cz_profile * max(1, 8 * count))()
+        a4 = (ct.c_uint32 * max(1, count))()
+        npr, nprof = ct.c_uint32(), ct.c_uint32()
+        rc = self.lib.cz_poll(self.h, rid, -1, ps, count, ct.byref(npr), out, 8 * count, ct.byref(nprof), a4)
+        if rc != 0:
+            raise CensusError(f"request {rid} refused (rc={rc}): "
+                              f"{self.lib.cz_server_last_error(self.h).decode(errors='replace')}")
+        primes = list(ps[:npr.value])
+        return primes, to_records(primes, out, list(a4[:npr.value]))
 
-    # -- trace replay ---------------------------------------------------------
     def run(self, requests: list) -> list:
-        """Serve a trace in real time (arrivals at their timestamps)."""
-        threads = [threading.Thread(target=self._slot_loop, args=(k,), daemon=True) for k in range(len(self.slots))]
+        """Serve a trace in real time: each request is submitted at its arrival
+        time; a collector thread takes completions as they happen."""
+        by_id, errors = {}, []
+        lock = threading.Lock()
+
+        def collect():
+            pending = len(requests)
+            while pending:
+                rid = self.next_done(50)
+                if rid is None:
+                    continue
+                now = time.perf_counter() - self.t0
+                with lock:
+                    r = by_id[rid]
+                try:
+                    r.primes, r.records = self.fetch(rid, r.count)
+                except Exception as e:              # a refused request fails the run
+                    errors.append(e)
+                r.done = now
+                pending -= 1
+
+        th = threading.Thread(target=collect, daemon=True)
         self.t0 = time.perf_counter()
-        for t in threads:
-            t.start()
+        th.start()
         for r in sorted(requests, key=lambda x: x.arrival):
             delay = r.arrival - (time.perf_counter() - self.t0)
             if delay > 0:
                 time.sleep(delay)
-            with self.cv:
-                if self.closed:
-                    break
-                self.waiting.append(r)
-                self.cv.notify()
-        with self.cv:
-            self.closed = True
-            self.cv.notify_all()
-        for t in threads:
-            t.join()
-        if self.error:
-            raise self.error
+            with lock:
+                by_id[self.submit(r.lo, r.count)] = r
+        th.join()
+        if errors:
+            raise errors[0]
         return requests
 
 

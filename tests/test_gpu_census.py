@@ -184,3 +184,15 @@ def test_speculation_miss_rerun_exact():
         got = tup(c1.profiles(ps, mode="sparse", a4=False))
         assert c1.last_stats["n_respec"] > 0
     assert got == want
+
+
+def test_refusal_leaves_no_stale_state(eng):
+    """A refused call (a composite: its A4 is not certified) followed, on the
+    same handle, by an all-dense call with A4 must succeed: no status of the
+    refused call survives into the next one."""
+    from rabung_atlas32_b200.census import CensusError
+    with pytest.raises(CensusError):
+        eng.profiles(sieve.primes_from(1 << 25, 4) + [(1 << 25) + 1], mode="auto", a4=True)
+    small = sieve.primes_in(3, 500)
+    got = eng.profiles(small, mode="auto", a4=True)
+    assert [r.a4 for r in got] == [oracle.a4(p) for p in small]

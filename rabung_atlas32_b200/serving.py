@@ -89,16 +89,21 @@ class Server:
         if rc != 0:
             raise RuntimeError(f"cz_server_open failed (rc={rc})")
         self.h = h
+        self._closed_batches = 0
         self.t0 = 0.0
 
     @property
     def batches(self) -> int:
+        """Batches run so far (the final count once the server is closed)."""
+        if self.h is None:
+            return self._closed_batches
         b = self._ct.c_uint64()
         self.lib.cz_server_info(self.h, self._ct.byref(b), None, None)
         return int(b.value)
 
     def close(self):
         if self.h is not None:
+            self._closed_batches = self.batches
             self.lib.cz_server_close(self.h)
             self.h = None
 

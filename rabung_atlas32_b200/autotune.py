@@ -65,6 +65,8 @@ def _measure(t: Tuning, primes, mode: str, reps: int = 2):
 
 def anchor_pref(r: int, bits: int) -> int:
     """Stages the filter derives from anchor_bits: least t with r^(t-1) >= 2^(5+bits)."""
+    if r < 2:
+        raise ValueError(f"order r = {r} has no anchor stages")
     k, pw = 0, 1
     while pw < 1 << (5 + bits):
         pw *= r

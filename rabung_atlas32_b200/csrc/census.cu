@@ -110,6 +110,10 @@ struct cz_handle {
     std::vector<OutRecord> hout;
     void *pin = nullptr;
     size_t pin_cap = 0;
+    Buf b_tex;                               // texture handles of the plane pool's 1 GiB chunks (uint4 texels)
+    std::vector<cudaTextureObject_t> tex;
+    void *tex_for = nullptr;
+    size_t tex_cap = 0;
 };
 
 namespace {
@@ -260,8 +264,11 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
                 D.D = Ds[k];
                 D.qspec = qspec_for(c, p, r, !(flags & CZ_NOSPEC));
                 D.tpref = c.anchor_t[r] ? c.anchor_t[r] : anchor_pref(r, c.anchor_bits);
-                D.plane_off = plane_words;              // multiple of 8 words: 256-bit loads align
-                plane_words += ((u64)D.npp * (P.nwords + P.nwords2) + 7ull) & ~7ull;
+                const u64 pw = ((u64)D.npp * (P.nwords + P.nwords2) + 7ull) & ~7ull;
+                // no profile block straddles a 1 GiB texture chunk of the pool
+                if ((plane_words >> 28) != ((plane_words + pw - 1ull) >> 28)) plane_words = ((plane_words >> 28) + 1ull) << 28;
+                D.plane_off = plane_words;              // multiple of 8 words: vector loads and texels align
+                plane_words += pw;
                 D.local = (u32)h->h_sidx.size() - 1u;
                 h->h_slist.push_back((u32)h->hprof.size());
             } else {
@@ -329,6 +336,30 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
         !ensure(h, h->b_a4, 4ull * n) ||
         !ensure(h, h->b_counter, 64))
         return CZ_ECUDA;
+    // linear uint4 textures over the plane pool, one per 1 GiB chunk (2^26
+    // texels, within the 1-D linear texture limit), rebuilt when the pool moves;
+    // the filter fetches its 4-plane windows through them
+    if (h->tex_for != h->b_planes.p || h->tex_cap != h->b_planes.cap) {
+        for (auto t : h->tex) cudaDestroyTextureObject(t);
+        h->tex.clear();
+        const size_t chunk = 1ull << 30;
+        for (size_t off = 0; off < h->b_planes.cap; off += chunk) {
+            cudaResourceDesc rd{};
+            rd.resType = cudaResourceTypeLinear;
+            rd.res.linear.devPtr = (char *)h->b_planes.p + off;
+            rd.res.linear.desc = cudaCreateChannelDesc<uint4>();
+            rd.res.linear.sizeInBytes = std::min(chunk, h->b_planes.cap - off) & ~(size_t)15;
+            cudaTextureDesc td{};
+            td.readMode = cudaReadModeElementType;
+            cudaTextureObject_t t = 0;
+            if (!ck(h, cudaCreateTextureObject(&t, &rd, &td, nullptr), "texture")) return CZ_ECUDA;
+            h->tex.push_back(t);
+        }
+        if (!ensure(h, h->b_tex, 8ull * h->tex.size())) return CZ_ECUDA;
+        cudaMemcpy(h->b_tex.p, h->tex.data(), 8ull * h->tex.size(), cudaMemcpyHostToDevice);
+        h->tex_for = h->b_planes.p;
+        h->tex_cap = h->b_planes.cap;
+    }
     h->flags = flags;
     h->have_plan = true;
     return CZ_OK;
@@ -409,6 +440,7 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
         sa.next = P<u32>(h->b_counter);
         sa.group = std::max(1u, h->cfg.cta_per_profile);
         sa.tune.screen = h->cfg.screen;
+        sa.tex4 = P<unsigned long long>(h->b_tex);
         u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : 2u * (u32)h->sms;
         grid = std::min(grid, h->nsl * sa.group);
         sparse_kernel<<<grid, SPARSE_WARPS * 32, 0, st>>>(sa);
@@ -560,6 +592,8 @@ void cz_close(cz_handle *h) {
     Buf *bufs[] = {&h->b_in, &h->b_primes, &h->b_profs, &h->b_state, &h->b_planes, &h->b_summ, &h->b_chunk,
                    &h->b_summp, &h->b_didx, &h->b_sidx, &h->b_slist, &h->b_dlist, &h->b_dpre, &h->b_out,
                    &h->b_a4, &h->b_counter, &h->b_sreq, &h->b_sout};
+    for (auto t : h->tex) cudaDestroyTextureObject(t);
+    if (h->b_tex.p) cudaFree(h->b_tex.p);
     for (Buf *b : bufs) if (b->p) cudaFree(b->p);
     if (h->pin) cudaFreeHost(h->pin);
     if (h->d_small) cudaFree(h->d_small);

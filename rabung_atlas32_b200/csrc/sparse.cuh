@@ -75,6 +75,7 @@ struct SparseArgs {
     u32 *next;                // work counter: CTA slots handed out
     u32 group;                // CTAs that share one profile (its rows)
     Tuning tune;
+    const unsigned long long *tex4;   // uint4 texture objects over 1 GiB chunks of the plane pool
 };
 
 struct Cand { u32 b, d; };
@@ -87,13 +88,6 @@ CZ_HD u32 anchor_pref(u32 r, u32 bits) {
     u32 k = 0;
     while (pw < goal) { pw *= r; ++k; }
     return k + 1u;
-}
-
-// 256-bit read-only load (sm_100), 32-byte aligned address
-__device__ __forceinline__ void ld_nc_256(const u32 *p, uint4 &lo, uint4 &hi) {
-    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(lo.x), "=r"(lo.y), "=r"(lo.z), "=r"(lo.w), "=r"(hi.x), "=r"(hi.y), "=r"(hi.z), "=r"(hi.w)
-        : "l"(p));
 }
 
 // windows of all NPP interleaved planes at bit index u
@@ -136,23 +130,6 @@ template <> struct Planes<4> {
         o[2] = __funnelshift_r(a.z, b.z, sh);
         o[3] = __funnelshift_r(a.w, b.w, sh);
     }
-    // the three plane groups of a 64-bit window from two aligned 256-bit
-    // loads (view bases are 32-byte aligned; the fourth group read lies in
-    // the view's padding)
-    static __device__ __forceinline__ void win64(const u32 *__restrict__ P, u32 u, u32 *lo, u32 *hi) {
-        const u32 wi = u >> 5;
-        const u32 *q = P + 8u * (wi >> 1);
-        uint4 x0, x1, y0, y1;
-        ld_nc_256(q, x0, x1);
-        ld_nc_256(q + 8, y0, y1);
-        const bool odd = wi & 1u;
-        const uint4 a = odd ? x1 : x0, b = odd ? y0 : x1, c = odd ? y1 : y0;
-        const u32 sh = u & 31u;
-        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
-        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
-        lo[2] = __funnelshift_r(a.z, b.z, sh); hi[2] = __funnelshift_r(b.z, c.z, sh);
-        lo[3] = __funnelshift_r(a.w, b.w, sh); hi[3] = __funnelshift_r(b.w, c.w, sh);
-    }
 };
 
 // mismatch mask of a window against the base windows
@@ -166,16 +143,6 @@ __device__ __forceinline__ u32 mismatch(const u32 *__restrict__ P, u32 u, const 
     return m;
 }
 
-// 64-bit mismatch mask (hi:lo) of a window against the base windows
-template <int NPP>
-__device__ __forceinline__ u64 mismatch64(const u32 *__restrict__ P, u32 u, const u32 *blo, const u32 *bhi) {
-    u32 lo[NPP], hi[NPP];
-    Planes<NPP>::win64(P, u, lo, hi);
-    u32 ml = lo[0] ^ blo[0], mh = hi[0] ^ bhi[0];
-#pragma unroll
-    for (int k = 1; k < NPP; ++k) { ml |= lo[k] ^ blo[k]; mh |= hi[k] ^ bhi[k]; }
-    return ((u64)mh << 32) | ml;
-}
 
 // one view of the signed table: index i <-> numerator c + G i, i in [ilo, ihi]
 struct View {
@@ -193,6 +160,8 @@ struct ProfCtx {
     u32 om[9];
     u32 seed, qspec;       // certified stretch from the table, speculative threshold
     u32 tpref;             // preferred anchor stages for this order
+    unsigned long long btex, otex;   // textures of the chunks holding the base / odd view
+    u32 btoff, otoff;                // uint4 element of each view's word 0 in its chunk
 };
 
 // colour of numerator n (|n| <= B) as an integer, from the base view
@@ -379,6 +348,41 @@ __device__ __forceinline__ void queue_words(const ProfCtx &c, uint4 *sb, Cand *c
     if (q.nscr >= 32u) screen_batch<NPP>(c, sb, cb, q, 32u, screen, st, lane);
 }
 
+// 64-bit window lo = bits [u, u+32), hi = bits [u+32, u+64) of a view.
+// 4-plane windows are fetched through the texture pipe of the L1 unit
+// (three uint4 texels from a linear texture over the plane pool; u then counts
+// from the texture chunk's element 0), the others through the load/store pipe:
+// the filter is bound by load/store wavefronts, and the texture pipe next to
+// it would otherwise stay idle, so the two kinds of profile stop competing
+// for one pipe.
+template <int NPP>
+__device__ __forceinline__ void win64(const View &v, unsigned long long tex, u32 u, u32 *lo, u32 *hi) {
+    if constexpr (NPP == 4) {
+        const int e = (int)(u >> 5);
+        const uint4 a = tex1Dfetch<uint4>(tex, e), b = tex1Dfetch<uint4>(tex, e + 1),
+                    c = tex1Dfetch<uint4>(tex, e + 2);
+        const u32 sh = u & 31u;
+        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
+        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
+        lo[2] = __funnelshift_r(a.z, b.z, sh); hi[2] = __funnelshift_r(b.z, c.z, sh);
+        lo[3] = __funnelshift_r(a.w, b.w, sh); hi[3] = __funnelshift_r(b.w, c.w, sh);
+    } else {
+        Planes<NPP>::win64(v.P, u, lo, hi);
+    }
+}
+
+// 64-bit mismatch mask (hi:lo) of a window against the base windows
+template <int NPP>
+__device__ __forceinline__ u64 mismatch64(const View &v, unsigned long long tex, u32 u, const u32 *blo,
+                                          const u32 *bhi) {
+    u32 lo[NPP], hi[NPP];
+    win64<NPP>(v, tex, u, lo, hi);
+    u32 ml = 0, mh = 0;
+#pragma unroll
+    for (int k = 0; k < NPP; ++k) { ml |= lo[k] ^ blo[k]; mh |= hi[k] ^ bhi[k]; }
+    return ((u64)mh << 32) | ml;
+}
+
 // all selected words of row d on view v, 64 anchors per lane-word: per stage
 // three plane words, two funnel shifts and two logic ops per plane test 64
 // anchors, so ALU work and L1 requests per anchor-stage drop against 32-bit
@@ -386,7 +390,7 @@ __device__ __forceinline__ void queue_words(const ProfCtx &c, uint4 *sb, Cand *c
 template <int NPP>
 __device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref, u32 d, u32 t, u32 s,
                                              const Tuning &tune, uint4 *sb, Cand *cb, WarpQ &q, ProfState *st,
-                                             int lane) {
+                                             int lane, unsigned long long tex = 0ull, u32 tbits = 0u) {
     const View v = vref;
     const u32 G = v.G, dd = d / G;
     const u32 beta = ((t - 1u) * d + 1u) >> 1;
@@ -416,16 +420,16 @@ __device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref,
         }
         if (alive) {
             ++q.words;
-            const u32 u = i0 + v.OFF;
+            const u32 u = i0 + v.OFF + tbits;        // tbits: texture chunk offset (4 planes), else 0
             u32 blo[NPP], bhi[NPP];
-            Planes<NPP>::win64(v.P, u, blo, bhi);
+            win64<NPP>(v, tex, u, blo, bhi);
             constexpr int SB = NPP == 4 ? CZ_SB4 : (NPP == 2 ? CZ_SB2 : CZ_SB1);
             u32 j = 1;
             while (j < t && alive) {
                 u64 m[SB];
 #pragma unroll
                 for (int k = 0; k < SB; ++k)
-                    m[k] = (j + (u32)k < t) ? mismatch64<NPP>(v.P, u - (j + (u32)k) * dd, blo, bhi) : 0ull;
+                    m[k] = (j + (u32)k < t) ? mismatch64<NPP>(v, tex, u - (j + (u32)k) * dd, blo, bhi) : 0ull;
 #pragma unroll
                 for (int k = 0; k < SB; ++k) alive &= ~m[k];
                 j += SB;
@@ -434,6 +438,32 @@ __device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref,
         }
         queue_words<NPP>(c, sb, cb, q, i0, (u32)alive, d, t, screen, st, lane);
         queue_words<NPP>(c, sb, cb, q, i0 + 32u, (u32)(alive >> 32), d, t, screen, st, lane);
+    }
+}
+
+// the rows of one profile, handed out one per warp in increasing d
+template <int NPP>
+__device__ __forceinline__ void filter_rows(const ProfCtx &c, const SparseArgs &a, u32 tpref, uint4 *sb, Cand *cb,
+                                            WarpQ &q, ProfState *st, int lane) {
+    for (;;) {
+        u32 d = 0;
+        if (lane == 0) d = atomicAdd(&st->rows_next, 1u) + 1u;     // rows in increasing d
+        d = __shfl_sync(0xFFFFFFFFu, d, 0);
+        if (d > c.D) break;
+        // row parameters from the verified maximum so far (<= M); with a
+        // speculative threshold every run >= it is still completed, and a
+        // profile whose best stays below it is re-run without it
+        const u32 blen = threshold(c, st);
+        const u32 q_ = blen < c.Q ? blen : c.Q;
+        if (q_ < 3u) { q.err |= 2u; break; }
+        const u32 t = tpref < q_ ? (tpref < 2u ? 2u : tpref) : q_;
+        const u32 s = q_ - t + 1u;
+        const View &v = (d & 1u) ? c.base : c.odd;
+        if constexpr (NPP == 4)
+            filter_row64<NPP>(c, v, d, t, s, a.tune, sb, cb, q, st, lane, (d & 1u) ? c.btex : c.otex,
+                              32u * ((d & 1u) ? c.btoff : c.otoff));
+        else
+            filter_row64<NPP>(c, v, d, t, s, a.tune, sb, cb, q, st, lane);
     }
 }
 
@@ -462,6 +492,14 @@ sparse_kernel(SparseArgs a) {
                 // odd view: n = 2i + 1 in [-B, B]  <=>  i in [ceil((-B-1)/2), floor((B-1)/2)]
                 c.odd = View{c.P + (size_t)PR.nwords * PD.npp, 32u * PR.K2, -(i32)((PR.B + 1u) / 2u),
                              (i32)((PR.B - 1u) / 2u), 2u, 1u};
+                {
+                    const u64 bb = (u64)PD.plane_off * 4ull;
+                    const u64 ob = bb + (u64)PR.nwords * PD.npp * 4ull;
+                    c.btex = __ldg(a.tex4 + (bb >> 30));
+                    c.btoff = (u32)((bb & ((1ull << 30) - 1ull)) >> 4);
+                    c.otex = __ldg(a.tex4 + (ob >> 30));
+                    c.otoff = (u32)((ob & ((1ull << 30) - 1ull)) >> 4);
+                }
                 for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
                 c.seed = *(volatile u32 *)&a.state[gprof].seed;
                 c.qspec = PD.qspec;
@@ -478,24 +516,10 @@ sparse_kernel(SparseArgs a) {
         WarpQ q{0, 0, 0, 0, 0, 0, 0};
         uint4 *sb = sbuf[warp];
         Cand *cb = cbuf[warp];
-        for (;;) {
-            u32 d = 0;
-            if (lane == 0) d = atomicAdd(&st->rows_next, 1u) + 1u;     // rows in increasing d
-            d = __shfl_sync(0xFFFFFFFFu, d, 0);
-            if (d > c.D) break;
-            // row parameters from the verified maximum so far (<= M); with a
-            // speculative threshold every run >= it is still completed, and a
-            // profile whose best stays below it is re-run without it
-            const u32 blen = threshold(c, st);
-            const u32 q_ = blen < c.Q ? blen : c.Q;
-            if (q_ < 3u) { q.err |= 2u; break; }
-            const u32 t = tpref < q_ ? (tpref < 2u ? 2u : tpref) : q_;
-            const u32 s = q_ - t + 1u;
-            const View &v = (d & 1u) ? c.base : c.odd;
-            if (c.npp == 1u) filter_row64<1>(c, v, d, t, s, a.tune, sb, cb, q, st, lane);
-            else if (c.npp == 2u) filter_row64<2>(c, v, d, t, s, a.tune, sb, cb, q, st, lane);
-            else filter_row64<4>(c, v, d, t, s, a.tune, sb, cb, q, st, lane);
-        }
+        // one row loop per stored plane count, so each keeps its own registers
+        if (c.npp == 1u) filter_rows<1>(c, a, tpref, sb, cb, q, st, lane);
+        else if (c.npp == 2u) filter_rows<2>(c, a, tpref, sb, cb, q, st, lane);
+        else filter_rows<4>(c, a, tpref, sb, cb, q, st, lane);
         // the screen queue carries across rows: drain it, then the candidates
         if (q.nscr) {
             if (c.npp == 1u) screen_batch<1>(c, sb, cb, q, q.nscr, a.tune.screen != 0u, st, lane);

@@ -110,10 +110,11 @@ struct cz_handle {
     std::vector<OutRecord> hout;
     void *pin = nullptr;
     size_t pin_cap = 0;
-    Buf b_tex;                               // texture handles of the plane pool's 1 GiB chunks (uint4 texels)
+    Buf b_tex;                               // texture handles [texel format][pool chunk]
     std::vector<cudaTextureObject_t> tex;
     void *tex_for = nullptr;
     size_t tex_cap = 0;
+    u32 tex_chunks = 0;
 };
 
 namespace {
@@ -265,8 +266,9 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
                 D.qspec = qspec_for(c, p, r, !(flags & CZ_NOSPEC));
                 D.tpref = c.anchor_t[r] ? c.anchor_t[r] : anchor_pref(r, c.anchor_bits);
                 const u64 pw = ((u64)D.npp * (P.nwords + P.nwords2) + 7ull) & ~7ull;
-                // no profile block straddles a 1 GiB texture chunk of the pool
-                if ((plane_words >> 28) != ((plane_words + pw - 1ull) >> 28)) plane_words = ((plane_words >> 28) + 1ull) << 28;
+                // no profile block straddles a texture chunk of the pool
+                if ((plane_words >> TEX_CHUNK_WORDS_LOG2) != ((plane_words + pw - 1ull) >> TEX_CHUNK_WORDS_LOG2))
+                    plane_words = ((plane_words >> TEX_CHUNK_WORDS_LOG2) + 1ull) << TEX_CHUNK_WORDS_LOG2;
                 D.plane_off = plane_words;              // multiple of 8 words: vector loads and texels align
                 plane_words += pw;
                 D.local = (u32)h->h_sidx.size() - 1u;
@@ -336,25 +338,33 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
         !ensure(h, h->b_a4, 4ull * n) ||
         !ensure(h, h->b_counter, 64))
         return CZ_ECUDA;
-    // linear uint4 textures over the plane pool, one per 1 GiB chunk (2^26
-    // texels, within the 1-D linear texture limit), rebuilt when the pool moves;
-    // the filter fetches its 4-plane windows through them
+    // linear textures over the plane pool, one per chunk and texel format
+    // (uint, uint2, uint4 for 1, 2, 4 stored planes; a 512 MiB chunk holds at
+    // most 2^27 texels, within the 1-D linear texture limit), rebuilt when the
+    // pool moves; the filter fetches the windows of the plane counts in
+    // CZ_TEX_MASK through them
     if (h->tex_for != h->b_planes.p || h->tex_cap != h->b_planes.cap) {
         for (auto t : h->tex) cudaDestroyTextureObject(t);
         h->tex.clear();
-        const size_t chunk = 1ull << 30;
-        for (size_t off = 0; off < h->b_planes.cap; off += chunk) {
-            cudaResourceDesc rd{};
-            rd.resType = cudaResourceTypeLinear;
-            rd.res.linear.devPtr = (char *)h->b_planes.p + off;
-            rd.res.linear.desc = cudaCreateChannelDesc<uint4>();
-            rd.res.linear.sizeInBytes = std::min(chunk, h->b_planes.cap - off) & ~(size_t)15;
-            cudaTextureDesc td{};
-            td.readMode = cudaReadModeElementType;
-            cudaTextureObject_t t = 0;
-            if (!ck(h, cudaCreateTextureObject(&t, &rd, &td, nullptr), "texture")) return CZ_ECUDA;
-            h->tex.push_back(t);
-        }
+        const size_t chunk = (size_t)4 << TEX_CHUNK_WORDS_LOG2;
+        const size_t nch = (h->b_planes.cap + chunk - 1) / chunk;
+        const cudaChannelFormatDesc fmt[3] = {cudaCreateChannelDesc<unsigned int>(), cudaCreateChannelDesc<uint2>(),
+                                              cudaCreateChannelDesc<uint4>()};
+        for (int f = 0; f < 3; ++f)
+            for (size_t k = 0; k < nch; ++k) {
+                const size_t off = k * chunk;
+                cudaResourceDesc rd{};
+                rd.resType = cudaResourceTypeLinear;
+                rd.res.linear.devPtr = (char *)h->b_planes.p + off;
+                rd.res.linear.desc = fmt[f];
+                rd.res.linear.sizeInBytes = std::min(chunk, h->b_planes.cap - off) & ~(size_t)15;
+                cudaTextureDesc td{};
+                td.readMode = cudaReadModeElementType;
+                cudaTextureObject_t t = 0;
+                if (!ck(h, cudaCreateTextureObject(&t, &rd, &td, nullptr), "texture")) return CZ_ECUDA;
+                h->tex.push_back(t);
+            }
+        h->tex_chunks = (u32)nch;
         if (!ensure(h, h->b_tex, 8ull * h->tex.size())) return CZ_ECUDA;
         cudaMemcpy(h->b_tex.p, h->tex.data(), 8ull * h->tex.size(), cudaMemcpyHostToDevice);
         h->tex_for = h->b_planes.p;
@@ -440,7 +450,8 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
         sa.next = P<u32>(h->b_counter);
         sa.group = std::max(1u, h->cfg.cta_per_profile);
         sa.tune.screen = h->cfg.screen;
-        sa.tex4 = P<unsigned long long>(h->b_tex);
+        sa.texs = P<unsigned long long>(h->b_tex);
+        sa.tex_chunks = h->tex_chunks;
         u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : 2u * (u32)h->sms;
         grid = std::min(grid, h->nsl * sa.group);
         sparse_kernel<<<grid, SPARSE_WARPS * 32, 0, st>>>(sa);

@@ -57,6 +57,11 @@ namespace cz {
 #define CZ_SPARSE_MINB 2
 #endif
 
+#ifndef CZ_TEX_MASK                   // stored plane counts (bit NPP) whose windows go through textures
+#define CZ_TEX_MASK 4
+#endif
+constexpr u32 TEX_CHUNK_WORDS_LOG2 = 27;   // texture chunks of the plane pool: 2^27 words (512 MiB)
+
 constexpr int SPARSE_WARPS = 16;
 constexpr int CAND_CAP = 64;          // per-warp buffers
 constexpr u32 RUN_CAP = 4096;         // longest run a completion may walk
@@ -75,7 +80,8 @@ struct SparseArgs {
     u32 *next;                // work counter: CTA slots handed out
     u32 group;                // CTAs that share one profile (its rows)
     Tuning tune;
-    const unsigned long long *tex4;   // uint4 texture objects over 1 GiB chunks of the plane pool
+    const unsigned long long *texs;   // linear textures over the plane pool: [uint, uint2, uint4][chunk]
+    u32 tex_chunks;
 };
 
 struct Cand { u32 b, d; };
@@ -348,24 +354,47 @@ __device__ __forceinline__ void queue_words(const ProfCtx &c, uint4 *sb, Cand *c
     if (q.nscr >= 32u) screen_batch<NPP>(c, sb, cb, q, 32u, screen, st, lane);
 }
 
+// the NPP words of texel e of a linear texture whose texels hold NPP words
+template <int NPP> struct Texel;
+template <> struct Texel<1> {
+    static __device__ __forceinline__ void get(unsigned long long t, int e, u32 *w) {
+        w[0] = tex1Dfetch<unsigned int>(t, e);
+    }
+};
+template <> struct Texel<2> {
+    static __device__ __forceinline__ void get(unsigned long long t, int e, u32 *w) {
+        const uint2 x = tex1Dfetch<uint2>(t, e);
+        w[0] = x.x; w[1] = x.y;
+    }
+};
+template <> struct Texel<4> {
+    static __device__ __forceinline__ void get(unsigned long long t, int e, u32 *w) {
+        const uint4 x = tex1Dfetch<uint4>(t, e);
+        w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+    }
+};
+
 // 64-bit window lo = bits [u, u+32), hi = bits [u+32, u+64) of a view.
-// 4-plane windows are fetched through the texture pipe of the L1 unit
-// (three uint4 texels from a linear texture over the plane pool; u then counts
-// from the texture chunk's element 0), the others through the load/store pipe:
-// the filter is bound by load/store wavefronts, and the texture pipe next to
-// it would otherwise stay idle, so the two kinds of profile stop competing
-// for one pipe.
+// Windows of the plane counts in CZ_TEX_MASK are fetched through the texture
+// pipe of the L1 unit (three texels from a linear texture over the plane
+// pool; u then counts from the texture chunk's element 0), the others through
+// the load/store pipe: the filter is bound by load/store wavefronts, and the
+// texture pipe next to it would otherwise stay idle, so profiles of different
+// plane counts stop competing for one pipe.
 template <int NPP>
 __device__ __forceinline__ void win64(const View &v, unsigned long long tex, u32 u, u32 *lo, u32 *hi) {
-    if constexpr (NPP == 4) {
+    if constexpr ((CZ_TEX_MASK & NPP) != 0) {
         const int e = (int)(u >> 5);
-        const uint4 a = tex1Dfetch<uint4>(tex, e), b = tex1Dfetch<uint4>(tex, e + 1),
-                    c = tex1Dfetch<uint4>(tex, e + 2);
+        u32 a[NPP], b[NPP], c[NPP];
+        Texel<NPP>::get(tex, e, a);
+        Texel<NPP>::get(tex, e + 1, b);
+        Texel<NPP>::get(tex, e + 2, c);
         const u32 sh = u & 31u;
-        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
-        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
-        lo[2] = __funnelshift_r(a.z, b.z, sh); hi[2] = __funnelshift_r(b.z, c.z, sh);
-        lo[3] = __funnelshift_r(a.w, b.w, sh); hi[3] = __funnelshift_r(b.w, c.w, sh);
+#pragma unroll
+        for (int k = 0; k < NPP; ++k) {
+            lo[k] = __funnelshift_r(a[k], b[k], sh);
+            hi[k] = __funnelshift_r(b[k], c[k], sh);
+        }
     } else {
         Planes<NPP>::win64(v.P, u, lo, hi);
     }
@@ -459,7 +488,7 @@ __device__ __forceinline__ void filter_rows(const ProfCtx &c, const SparseArgs &
         const u32 t = tpref < q_ ? (tpref < 2u ? 2u : tpref) : q_;
         const u32 s = q_ - t + 1u;
         const View &v = (d & 1u) ? c.base : c.odd;
-        if constexpr (NPP == 4)
+        if constexpr ((CZ_TEX_MASK & NPP) != 0)
             filter_row64<NPP>(c, v, d, t, s, a.tune, sb, cb, q, st, lane, (d & 1u) ? c.btex : c.otex,
                               32u * ((d & 1u) ? c.btoff : c.otoff));
         else
@@ -495,10 +524,12 @@ sparse_kernel(SparseArgs a) {
                 {
                     const u64 bb = (u64)PD.plane_off * 4ull;
                     const u64 ob = bb + (u64)PR.nwords * PD.npp * 4ull;
-                    c.btex = __ldg(a.tex4 + (bb >> 30));
-                    c.btoff = (u32)((bb & ((1ull << 30) - 1ull)) >> 4);
-                    c.otex = __ldg(a.tex4 + (ob >> 30));
-                    c.otoff = (u32)((ob & ((1ull << 30) - 1ull)) >> 4);
+                    const u32 f = PD.npp == 1u ? 0u : (PD.npp == 2u ? 1u : 2u), sh = TEX_CHUNK_WORDS_LOG2 + 2u;
+                    const u64 msk = (1ull << sh) - 1ull, tb = 4ull * PD.npp;   // bytes per texel
+                    c.btex = __ldg(a.texs + f * a.tex_chunks + (bb >> sh));
+                    c.btoff = (u32)((bb & msk) / tb);
+                    c.otex = __ldg(a.texs + f * a.tex_chunks + (ob >> sh));
+                    c.otoff = (u32)((ob & msk) / tb);
                 }
                 for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
                 c.seed = *(volatile u32 *)&a.state[gprof].seed;

@@ -45,7 +45,7 @@
 namespace cz {
 
 #ifndef CZ_SB1                       // anchor stages whose loads issue together, by stored planes
-#define CZ_SB1 4
+#define CZ_SB1 5                     // r = 2 runs t - 1 = 10 stages: two batches of 5
 #endif
 #ifndef CZ_SB2
 #define CZ_SB2 2

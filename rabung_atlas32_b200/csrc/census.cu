@@ -452,7 +452,7 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
         sa.tune.screen = h->cfg.screen;
         sa.texs = P<unsigned long long>(h->b_tex);
         sa.tex_chunks = h->tex_chunks;
-        u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : 2u * (u32)h->sms;
+        u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : (u32)CZ_SPARSE_MINB * (u32)h->sms;
         grid = std::min(grid, h->nsl * sa.group);
         sparse_kernel<<<grid, SPARSE_WARPS * 32, 0, st>>>(sa);
         ++launches;

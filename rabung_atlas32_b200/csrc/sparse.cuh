@@ -62,7 +62,10 @@ namespace cz {
 #endif
 constexpr u32 TEX_CHUNK_WORDS_LOG2 = 27;   // texture chunks of the plane pool: 2^27 words (512 MiB)
 
-constexpr int SPARSE_WARPS = 16;
+#ifndef CZ_SPARSE_WARPS               // warps per filter CTA
+#define CZ_SPARSE_WARPS 16
+#endif
+constexpr int SPARSE_WARPS = CZ_SPARSE_WARPS;
 constexpr int CAND_CAP = 64;          // per-warp buffers
 constexpr u32 RUN_CAP = 4096;         // longest run a completion may walk
 

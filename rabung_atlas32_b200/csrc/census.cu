@@ -448,11 +448,13 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
         sa.prof_list = P<u32>(h->b_slist);
         sa.nlist = h->nsl;
         sa.next = P<u32>(h->b_counter);
-        sa.group = std::max(1u, h->cfg.cta_per_profile);
+        u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : (u32)CZ_SPARSE_MINB * (u32)h->sms;
+        // a call with few profiles spreads each profile's rows over more CTAs
+        // (up to 64), so small calls fill the GPU; large calls keep the tuned group
+        sa.group = std::max(std::max(1u, h->cfg.cta_per_profile), std::min(64u, grid / std::max(1u, h->nsl)));
         sa.tune.screen = h->cfg.screen;
         sa.texs = P<unsigned long long>(h->b_tex);
         sa.tex_chunks = h->tex_chunks;
-        u32 grid = h->cfg.sparse_blocks ? h->cfg.sparse_blocks : (u32)CZ_SPARSE_MINB * (u32)h->sms;
         grid = std::min(grid, h->nsl * sa.group);
         sparse_kernel<<<grid, SPARSE_WARPS * 32, 0, st>>>(sa);
         ++launches;

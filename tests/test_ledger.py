@@ -146,3 +146,61 @@ def test_cli_verify_and_status(tmp_path, blocks):
                              cwd=ROOT, capture_output=True, text=True, check=True).stdout
         d = json.loads(out)
         assert str(d["next_lo"]) == "38891"
+
+
+class FakeCensus:
+    """Stands in for the GPU census on CPU: records of the reference's block 0
+    (decoded from the golden frames) and a host sieve.  `planted` changes the
+    dense re-check of one prime, as a faulty census would."""
+
+    def __init__(self, blocks, planted=None):
+        self.recs = {r.p: r for r in blocks["00000"][0]}
+        self.planted = planted
+        self.calls = []
+
+    def sieve(self, requests):
+        from rabung_atlas32_b200 import sieve
+        return [sieve.primes_from(lo, n) for lo, n in requests]
+
+    def profiles(self, primes, mode="auto", a4=True):
+        import copy
+        self.calls.append(mode)
+        out = [copy.deepcopy(self.recs[p]) for p in primes]
+        for r in out:
+            if mode == "dense" and r.p == self.planted:
+                r.profiles[0].M += 1
+            if not a4:
+                r.a4 = 0
+        return out
+
+
+def test_supervisor_cuts_blocks_resumes_and_audits(tmp_path, blocks):
+    fake = FakeCensus(blocks)
+    with ledger.Atlas(tmp_path) as at:
+        first = ledger.run(at, fake, 1, 38891, block_primes=1000, audit_every=2, max_blocks=2, log=lambda s: None)
+        assert [d["primes"] for d in first] == [1000, 1000]
+    with ledger.Atlas(tmp_path) as at:                                # resumes at next_lo
+        rest = ledger.run(at, fake, 1, 38891, block_primes=1000, audit_every=2, log=lambda s: None)
+        assert rest[0]["lo"] == first[-1]["hi"] and [d["primes"] for d in rest] == [1000, 1000, 96]
+        assert rest[-1]["hi"] == 38891
+        res = at.verify()
+        assert res["primes"] == 4096 and res["GPU_audits"] == res["A4_certificate_audits"] == 3
+        got = [r.p for b in range(5) for r in codec.decode_scan_frame(at.frame("scan", b))[0]]
+        assert got == [r.p for r in blocks["00000"][0]]
+    # a whole-block run reproduces the sample frames
+    with ledger.Atlas(tmp_path / "one") as at:
+        ledger.run(at, FakeCensus(blocks), 1, 38891, audit_every=1, log=lambda s: None)
+        assert at.frame("scan", 0) == (GOLDEN / "scan-00000.vdw").read_bytes()
+        assert at.frame("quadruplets", 0) == (GOLDEN / "quadruplets-00000.a4").read_bytes()
+
+
+def test_supervisor_stops_before_committing_a_failed_audit(tmp_path, blocks):
+    # every prime of the first block is in the audit sample when it holds 8 primes
+    recs = blocks["00000"][0]
+    fake = FakeCensus(blocks, planted=recs[3].p)
+    with ledger.Atlas(tmp_path) as at:
+        with pytest.raises(ledger.LedgerError, match="audit failed"):
+            ledger.run(at, fake, 1, 38891, block_primes=8, audit_every=1, audit_primes=8, log=lambda s: None)
+        assert at.next_lo == 1 and at.next_block == 0
+    with ledger.Atlas(tmp_path) as at:
+        assert at.recovered == [] and at.verify()["blocks"] == 0

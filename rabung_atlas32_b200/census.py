@@ -156,16 +156,29 @@ class Census:
 
     def interval(self, lo: int, hi: int, mode: str = "auto", a4: bool = True, max_primes: int = 1 << 20):
         """(primes, records) of every prime in [lo, hi): device sieve + census
-        in one library call (cz_census_interval)."""
-        cap = max(1, min(int(max_primes), 1 << 24))
-        ps = (ctypes.c_uint32 * cap)()
-        npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
-        out = (_lib.cz_profile * (8 * cap))()
-        a4buf = (ctypes.c_uint32 * cap)() if a4 else None
+        in one library call (cz_census_interval).  Buffers are sized from a
+        prime-count estimate; when it is short, the library reports the
+        exact counts and the call is repeated once with them.  More than
+        max_primes primes in the interval is an error."""
+        import math
+        lo, hi = int(lo), int(hi)
+        est = int((hi - lo) / max(1.0, math.log(max(lo, 3))) * 1.25) + 64
+        cap = max(1, min(int(max_primes), est))
+        out_cap = 8 * cap
         flags = MODES[mode] | (_lib.CZ_A4 if a4 else 0)
-        st = _lib.cz_stats()
-        rc = self.lib.cz_census_interval(self.h, int(lo), int(hi), flags, ps, cap, ctypes.byref(npr), out, 8 * cap,
-                                         ctypes.byref(nprof), a4buf, ctypes.byref(st))
+        for attempt in range(2):
+            ps = (ctypes.c_uint32 * cap)()
+            npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
+            out = (_lib.cz_profile * max(1, out_cap))()
+            a4buf = (ctypes.c_uint32 * cap)() if a4 else None
+            st = _lib.cz_stats()
+            rc = self.lib.cz_census_interval(self.h, lo, hi, flags, ps, cap, ctypes.byref(npr), out, out_cap,
+                                             ctypes.byref(nprof), a4buf, ctypes.byref(st))
+            if rc == _lib.CZ_ELIMIT and attempt == 0 and npr.value <= max_primes:
+                cap = max(1, npr.value)
+                out_cap = max(nprof.value, 8 * cap)
+                continue
+            break
         if rc != 0:
             raise CensusError(f"interval census refused (rc={rc}, primes {npr.value}): {self._err()}")
         self.last_stats = st.as_dict()

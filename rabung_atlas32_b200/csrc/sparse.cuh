@@ -18,8 +18,9 @@
 //    The anchors of a primitive row share gcd(b, d) = 1, so for even d only odd
 //    b are enumerated, on the odd-numerator view of the table (the reference's
 //    G = 2 wheel, PBV/src/wheel_filter.hpp:14-46).
-//  * Filter (PBV/src/wheel_filter.hpp:52-91): 32 anchors per word; a candidate
-//    survives while every anchor offset agrees with b on every colour plane.
+//  * Filter (PBV/src/wheel_filter.hpp:52-91): a candidate anchor survives while
+//    every offset b - jd (j < t) agrees with b on every colour plane; here 64
+//    anchors per lane-word, their stages in batches whose loads issue together.
 //  * Bilateral screen (B1/src/two_cuts.hpp:27-74): reject only when known
 //    mismatches on both sides bound the run below the verified maximum;
 //    numerators outside [-B, B] are unknown and never reject.
@@ -31,14 +32,18 @@
 //    processed with a fixed q <= (a verified run length) <= M, so every maximum
 //    run (or its reflection) is completed.
 //
-// B200 design: one persistent kernel; a CTA owns one (p, r) profile at a time
-// (its planes stay hot in that SM's L1 and in L2), its warps pull rows d in
-// increasing order from a shared-memory counter and re-read the verified
-// maximum at every row, so the threshold rises while the profile runs; lanes
-// take consecutive words of a row (one vector load fetches all interleaved
-// planes of a word, funnel shifts cut the windows); words that survive the
-// anchor are queued per warp (across rows) and screened 32 at a time, one per
-// lane, and the screened candidates are completed 32 at a time, one per lane.
+// B200 design: one persistent kernel over all profiles of a call, handed out
+// longest first; a group of CTAs (2 for large calls, up to 64 when a call has
+// few profiles) shares one (p, r) profile, its warps pull rows d in increasing
+// order from the profile's counter in global memory and re-read the verified
+// maximum at every row, so the threshold rises while the profile runs; each
+// stored plane count has its own row loop (its own registers); lanes take
+// consecutive 64-anchor words of a row, a window is cut from three plane words
+// by funnel shifts, fetched through the load/store pipe for 1 and 2 planes and
+// through the texture pipe (linear textures over the plane pool) for 4 planes,
+// so the two L1 pipes share the load; words that survive are queued per warp
+// (across rows) and screened 32 at a time, one per lane, and the screened
+// candidates are completed 32 at a time, one per lane.
 #pragma once
 #include "labels.cuh"
 

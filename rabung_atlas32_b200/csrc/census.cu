@@ -9,7 +9,10 @@
 //   finalize_kernel: prefix, optional direct certification, K, records;
 //   a4_kernel: quadratic A4 counts.
 // The device work of the last call can be replayed on resident inputs
-// (cz_replay), optionally through a captured CUDA graph.
+// (cz_replay), optionally through a captured CUDA graph.  The plane pool is
+// also bound to linear textures (one per 512 MiB chunk and texel format) for
+// the filter's texture-pipe loads.  runtime.cuh, included at the end, adds the
+// interval census and the serving runtime on top of these entry points.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>

@@ -27,9 +27,13 @@
 //    +31 centring), the positive half is the previous step's ballot shifted
 //    by one with this step's first bit on top; two steps make one odd-view
 //    word per sign;
-//  * the same pass records the longest monochromatic stretch inside [1, B] per
-//    profile: a real run length, hence a certified lower bound on M (the role
-//    of the reference's seed_runs/finish_seed, small_table.cuh:64-136).
+//  * the same pass records the longest monochromatic stretch inside [1, B] of
+//    each profile planned without a speculative threshold: a real run length,
+//    hence a certified lower bound on M (the role of the reference's
+//    seed_runs/finish_seed, small_table.cuh:64-136); a speculated profile is
+//    certified by its best run reaching the speculative threshold instead;
+//  * the planes of one numerator step are stored with one instruction per
+//    word kind, lane b holding plane b.
 #pragma once
 #include "labels.cuh"
 

@@ -8,18 +8,28 @@ every prime, through the certified rational-anchor filter.  Metric: profiles/s.
 
   value     device throughput with the inputs resident in HBM: K replays of
             the captured device work (CUDA graph), timed with CUDA events on
-            the library's own stream, L2 flushed between steps;
-  e2e       the same census through the public C ABI (cz_census) from host
-            buffers: planning, pinned host->device copies, kernels and the
-            device->host read of every record, timed per step on the host;
+            the library's own stream, L2 flushed between steps; every step
+            certifies every record on the device (witness run monochromatic
+            and closed at both ends, prefix, by direct powers), as the
+            reference worker does before it emits a record;
+  e2e       the same certified census through the public C ABI (cz_census)
+            from host buffers: planning, pinned host->device copies, kernels
+            and the device->host read of every record, timed per step on the
+            host;
   roofline  dominant kernel (sparse_kernel): plane-window comparisons per second
             against this GPU's measured integer-ALU peak for the same
             operation (cz_microbench);
   cpu_baseline / --impl reference
-            the reference's own CPU sparse engine (`advance adaptive p r 64 3 1`)
-            and A4 worker (`moment_worker`), built from its sources into
-            oracle/_ref, on a seeded bounded sample of the same workload, on all
-            host cores.
+            the reference's own CPU sparse engines -- `target p c f 64 1 8192 1`
+            for the coupled order pairs {2, 4} and {3, 6}, `advance adaptive
+            p r 64 3 1` for every other order -- and its A4 worker
+            (`moment_worker`), built from its sources into oracle/_ref, on a
+            seeded sample of whole primes of the same workload (every
+            admissible order of each, >= 256 profiles), on all host cores;
+  c4, c5    (one GPU, unless --quick) the batched uneven census of 64 blocks
+            of 4096 primes against one block per call, and the serving stream
+            of 10,000 requests against plain per-request calls, each with its
+            own clock record.
 
 Multi-GPU (torchrun): every rank censuses its own 4096-prime block (rank k
 takes the 4096 primes below rank k-1's block): independent blocks, no
@@ -58,18 +68,17 @@ def uneven_blocks(rank: int = 0, nblocks: int = 64, size: int = BLOCK, seed: int
     return [sieve.primes_from(s, size) for s in starts]
 
 
-def uneven_arm(args) -> None:
-    """Batched uneven census: all blocks in one call (persistent kernels, waves
-    when the plane pool exceeds its budget) vs one block per call."""
-    from rabung_atlas32_b200.census import Census
+def c4_measure(eng, steps: int, warmup: int) -> dict:
+    """C4: 64 uneven blocks in one certified call (persistent kernels, waves
+    when the plane pool exceeds its budget) against one block per call, same
+    GPU, records compared bit for bit."""
     blocks = uneven_blocks(int(os.environ.get("RANK", "0")))
     flat = [p for b in blocks for p in b]
-    eng = Census()
     nprof = eng.count_profiles(flat)
-    for _ in range(max(1, args.warmup - 2)):
+    for _ in range(max(1, warmup)):
         eng.raw(flat, mode="auto", a4=True)
     dev, e2e, waves = [], [], 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         t0 = time.perf_counter()
         out, a4, st = eng.raw(flat, mode="auto", a4=True)
         e2e.append(time.perf_counter() - t0)
@@ -85,13 +94,24 @@ def uneven_arm(args) -> None:
         plain_rec += [(x.p, x.r, x.M, x.L, x.witness) for x in o[:eng.count_profiles(b)]]
         plain_a4 += a
     same = batched == plain_rec + [tuple(plain_a4)]
-    print(json.dumps({
+    mean_dev = sum(dev) / len(dev)
+    return {
         "metric": "profiles/s, batched uneven census (64 blocks x 4096 primes, log-uniform starts in [2^16, 2^32))",
-        "value": round(nprof / (sum(dev) / len(dev)), 1), "unit": "profiles/s", "steps": args.steps,
+        "value": round(nprof / mean_dev, 1), "unit": "profiles/s", "steps": steps,
         "primes": len(flat), "profiles": nprof, "waves": waves,
         "e2e": round(nprof / (sum(e2e) / len(e2e)), 1),
         "plain_one_block_per_call": {"value": round(nprof / plain_dev, 1), "e2e": round(nprof / plain_e2e, 1)},
-        "batched_over_plain": round(plain_dev / (sum(dev) / len(dev)), 3), "bit_identical": same}))
+        "batched_over_plain": round(plain_dev / mean_dev, 3), "bit_identical": same}
+
+
+def uneven_arm(args) -> None:
+    from rabung_atlas32_b200.census import Census
+    with Census() as eng:
+        clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+        clk.start()
+        res = c4_measure(eng, args.steps, args.warmup)
+        res["clocks"] = clk.stop()
+    print(json.dumps(res))
 
 
 def max_over_ranks(values: list, dist=None, device=None) -> list:
@@ -188,35 +208,68 @@ def ref_bin(name: str) -> Path:
 
 
 def reference_available() -> str | None:
-    for n in ("advance", "moment_worker"):
+    for n in ("advance", "target", "moment_worker"):
         if not ref_bin(n).exists():
             return f"oracle/_ref/{n} not built (make -f oracle/Makefile.ref)"
     return None
 
 
-def reference_sample(primes: list, n_profiles: int, seed: int = 20261203) -> list:
+def reference_jobs(primes: list, min_profiles: int = 256, seed: int = 20261203) -> tuple:
+    """A seeded sample of whole primes of the workload (every admissible order
+    of each) holding at least min_profiles profiles, as reference CPU jobs:
+    ("target", p, c, f) for the coupled pairs {2, 4} and {3, 6} (the
+    reference's coupled engine), ("advance", p, r, 0) for every other order.
+    Returns (jobs, primes, profiles)."""
     rng = random.Random(seed)
-    pairs = [(p, r) for p in primes for r in range(2, 10) if (p - 1) % r == 0]
-    return sorted(rng.sample(pairs, min(n_profiles, len(pairs))))
+    order = list(primes)
+    rng.shuffle(order)
+    jobs, picked, nprof = [], [], 0
+    for p in order:
+        if nprof >= min_profiles:
+            break
+        rs = [r for r in range(2, 10) if (p - 1) % r == 0]
+        nprof += len(rs)
+        picked.append(p)
+        for c, f in ((2, 4), (3, 6)):
+            if c in rs and f in rs:
+                jobs.append(("target", p, c, f))
+                rs = [r for r in rs if r not in (c, f)]
+        jobs += [("advance", p, r, 0) for r in rs]
+    # longest jobs first, so the pool's tail is short
+    jobs.sort(key=lambda j: (j[0] != "target", j[1]))
+    return jobs, sorted(picked), nprof
 
 
-def run_reference_step(pairs: list, cores: int) -> tuple:
-    """Reference CPU census of a sample: sparse engine per (p, r) + A4 per prime,
-    one process per core; returns (seconds, results)."""
-    def one(pr):
-        p, r = pr
+def run_reference_step(jobs: list, primes: list, cores: int) -> tuple:
+    """Reference CPU census of a sample, one process per core: the sparse
+    engines per job plus moment_worker A4 of the sample's primes; returns
+    (seconds, records [p, r, M, L, witness])."""
+    def one(job):
+        kind, p, r, f = job
+        if kind == "target":
+            out = subprocess.run([str(ref_bin("target")), str(p), str(r), str(f), "64", "1", "8192", "1"],
+                                 capture_output=True, text=True, check=True).stdout
+            j = json.loads(out)
+            return [(p, r, j["coarse_maximum"], j["coarse_prefix"], j["coarse_witness"]),
+                    (p, f, j["fine_maximum"], j["fine_prefix"], j["fine_witness"])]
         out = subprocess.run([str(ref_bin("advance")), "adaptive", str(p), str(r), "64", "3", "1"],
                              capture_output=True, text=True, check=True).stdout
         j = json.loads(out)
-        return (p, r, j["maximum"], j["prefix"], j["witness"])
+        return [(p, r, j["maximum"], j["prefix"], j["witness"])]
 
-    primes = sorted({p for p, _ in pairs})
     t0 = time.perf_counter()
     with ThreadPoolExecutor(cores) as ex:
-        res = list(ex.map(one, pairs))
+        res = [v for part in ex.map(one, jobs) for v in part]
     line = f"0 -1 {len(primes)} " + " ".join(map(str, primes)) + "\nQUIT\n"
     subprocess.run([str(ref_bin("moment_worker"))], input=line.encode(), capture_output=True, check=True)
-    return time.perf_counter() - t0, res
+    return time.perf_counter() - t0, sorted(res)
+
+
+def reference_sample_text(jobs: list, primes: list, nprof: int) -> str:
+    nt = sum(1 for j in jobs if j[0] == "target")
+    return (f"{len(primes)} seeded whole primes of the top block, {nprof} profiles per step: {nt} coupled "
+            f"pairs by `target p c f 64 1 8192 1`, {len(jobs) - nt} orders by `advance adaptive p r 64 3 1`, "
+            f"moment_worker A4 of the {len(primes)} primes")
 
 
 def reference_arm(args) -> None:
@@ -229,24 +282,24 @@ def reference_arm(args) -> None:
         return
     cores = os.cpu_count() or 1
     primes = workload(0)
-    pairs = reference_sample(primes, max(16, min(256, 2 * cores)))
+    jobs, sp, nprof = reference_jobs(primes)
+    wjobs, wsp, _ = reference_jobs(primes, min_profiles=16, seed=1)
     for _ in range(args.warmup):
-        run_reference_step(pairs[: max(1, len(pairs) // 4)], cores)
+        run_reference_step(wjobs, wsp, cores)
     secs = []
     for _ in range(args.steps):
-        s, _ = run_reference_step(pairs, cores)
-        secs.append(s)
+        s_, _ = run_reference_step(jobs, sp, cores)
+        secs.append(s_)
     total = sum(secs)
-    value = len(pairs) * args.steps / total
-    sample = (f"{len(pairs)} seeded (p, r) pairs of the top block per step (advance adaptive p r 64 3 1) "
-              f"+ moment_worker A4 of their {len({p for p, _ in pairs})} primes")
+    value = nprof * args.steps / total
+    sample = reference_sample_text(jobs, sp, nprof)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "profiles/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000 * total / args.steps, 2), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "deterministic: the top block's own primes",
         "config": {"workload": "top block: 4096 consecutive primes ending at 4294967291, all admissible r",
-                   "primes": BLOCK, "sample_profiles": len(pairs), "parallelism": "host processes"},
+                   "primes": BLOCK, "sample_profiles": nprof, "parallelism": "host processes"},
         "cpu_baseline": {"value": round(value, 2), "unit": "profiles/s", "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": round(value, 2), "unit": "profiles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -264,6 +317,7 @@ def main():
     ap.add_argument("--workload", default="top", choices=["top", "uneven", "serve", "small"])
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--rate", type=float, default=40.0, help="offered load, requests/s (serve)")
+    ap.add_argument("--quick", action="store_true", help="top block only: no C4 / C5 sub-objects")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -278,7 +332,11 @@ def main():
         return
     if args.workload == "serve":
         from rabung_atlas32_b200 import serving
-        print(json.dumps(serving.benchmark(requests=args.requests, rate=args.rate, seed=20261203)))
+        clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+        clk.start()
+        res = serving.benchmark(requests=args.requests, rate=args.rate, seed=20261203)
+        res["clocks"] = clk.stop()
+        print(json.dumps(res))
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -356,13 +414,18 @@ def main():
                 "peak_source": "measured on this GPU by cz_microbench kind 0 (MEASURED_PEAKS.json holds no integer peak)",
                 "montgomery_peak_per_s": peak_mont,
                 "kernel_ms": {k: round(kstats[k], 3) for k in ("ms_setup", "ms_table", "ms_sparse", "ms_dense",
-                                                               "ms_a4", "ms_finalize")}}
-        prof_path = ROOT / "profiles" / "sparse_kernel_top_block.txt"
+                                                               "ms_a4", "ms_finalize")},
+                "certification": "every record certified on the device in each step (finalize_kernel: witness "
+                                 "run and its two ends by direct powers, prefix; its time is ms_finalize)"}
+        # DRAM traffic of one full-size sparse_kernel launch, from the committed
+        # ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum)
+        prof_path = ROOT / "profiles" / "sparse_kernel_dram_top_block.txt"
         if prof_path.exists():
             for line in prof_path.read_text().splitlines():
                 if line.startswith("dram_bytes_per_launch:"):
                     try:
                         roof["traffic"] = int(line.split(":")[1].split()[0])
+                        roof["traffic_source"] = "ncu, full 4096-prime launch (" + prof_path.name + ")"
                     except ValueError:
                         pass
         # plain form: one prime per call (the reference worker's per-prime launches)
@@ -398,12 +461,23 @@ def main():
                 out["cpu_baseline"] = {"value": None, "unavailable": why}
             else:
                 cores = os.cpu_count() or 1
-                pairs = reference_sample(primes, max(16, min(256, 2 * cores)))
-                secs, _ = run_reference_step(pairs, cores)
-                out["cpu_baseline"] = {"value": round(len(pairs) / secs, 2), "unit": "profiles/s", "cores": cores,
-                                       "kind": "reference",
-                                       "sample": f"{len(pairs)} seeded (p, r) pairs of the workload, "
-                                                 f"advance adaptive p r 64 3 1 + moment_worker A4"}
+                jobs, sp, nref = reference_jobs(primes)
+                secs, _ = run_reference_step(jobs, sp, cores)
+                out["cpu_baseline"] = {"value": round(nref / secs, 2), "unit": "profiles/s", "cores": cores,
+                                       "kind": "reference", "sample": reference_sample_text(jobs, sp, nref)}
+        if world == 1 and not args.quick:
+            # C4 and C5 on the same GPU, each with its own clock record
+            ck = ClockSampler(local)
+            ck.start()
+            c4 = c4_measure(eng, steps=2, warmup=1)
+            c4["clocks"] = ck.stop()
+            out["c4"] = c4
+            from rabung_atlas32_b200 import serving
+            ck = ClockSampler(local)
+            ck.start()
+            c5 = serving.benchmark(requests=args.requests, rate=args.rate, seed=20261203)
+            c5["clocks"] = ck.stop()
+            out["c5"] = c5
         print(json.dumps(out), flush=True)
     if dist:
         barrier()

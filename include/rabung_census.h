@@ -141,24 +141,27 @@ int cz_a4(cz_handle *h, const uint32_t *primes, uint32_t n, uint32_t *a4_out);
 int cz_microbench(cz_handle *h, uint32_t kind, double *per_second);
 
 /* Dense census that allocates no memory (no counterpart in the reference).
- * For callers that cannot call cudaMalloc -- code running inside a CUDA graph
- * capture into a pool it does not own, plugins in a host process that owns the
- * device memory budget, allocator-free services.  All device scratch is one
- * fixed 2 MiB array inside the library, held by every GPU that loads the
- * library until the process exits.  Limits: n <= 64 primes, each p < 4,194,304
+ * For callers that cannot call cudaMalloc: plugins inside a host process that
+ * owns the device memory budget, and allocator-free services that must not
+ * grow their device footprint after start-up.  All device scratch is one fixed
+ * 2 MiB array inside the library, held by every GPU that loads the library
+ * until the process exits.  Limits: n <= 64 primes, each p < 4,194,304
  * (CZ_ELIMIT beyond them).  primes and out are host arrays as in cz_census
  * (out holds cz_count_profiles() records); stream is a cudaStream_t (NULL for
- * the legacy default stream) on the current device; the call returns after
- * that stream has finished.  The first call on a device resolves the array's
- * device address and should come before any stream capture.  Calls share the
- * array: calls that overlap on the GPU race. */
+ * the legacy default stream) on the current device.  The call is synchronous:
+ * it returns after that stream has finished.  Every call resolves the array's
+ * device address for the current device (also after a cudaDeviceReset).  Calls
+ * share the array: calls that overlap on the GPU race. */
 int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_profile *out, uint32_t out_cap,
                             void *stream);
 
-/* Reference-compatible adapter (src/census/engine32/src/baseline_bridge.cu:7,21-27):
- * profile of one prime for the orders in `mask` (bit r-2), M into out[r] and
- * L into prefix[r] (arrays of >= 10).  Returns 0, or 2 when mask asks for an
- * order that does not divide p-1.  Not thread-safe (one global handle). */
+/* Number of primes in [lo, hi) (hi <= 2^33), computed exactly on the host:
+ * a segmented sieve for short intervals, else pi(hi-1) - pi(lo-1) by the
+ * Lucy-Hedgehog recursion (O(x^(3/4)), ~30 ms at 2^32).  Sizes interval
+ * buffers in one pass; replaces the reference's Meissel-Lehmer count,
+ * src/census/prime_count.cpp:11-24.  Needs no GPU. */
+uint64_t cz_prime_count(uint64_t lo, uint64_t hi);
+
 /* Census of every prime in [lo, hi) (hi <= 2^32): the primes are found by the
  * device sieve, then censused as by cz_census.  primes_out (capacity
  * primes_cap) receives them ascending and *n_primes their count; out
@@ -204,6 +207,16 @@ int cz_poll(cz_server *s, uint64_t request_id, int32_t timeout_ms, uint32_t *pri
 int cz_server_info(cz_server *s, uint64_t *batches, uint64_t *completed, uint64_t *waiting);
 const char *cz_server_last_error(cz_server *s);
 
+/* Reference-compatible adapter (src/census/engine32/src/baseline_bridge.cu:7,21-27):
+ * profile of one prime for the orders in `mask` (bit r-2), M into out[r] and
+ * L into prefix[r] (arrays of >= 10).  With full = 0 only the masks the
+ * reference serves without `full` are accepted -- 1 {2}, 5 {2,4}, 18 {3,6},
+ * 19 {2,3,6}, 23 {2,3,4,6} -- and any other mask returns 2, as there; with
+ * full = 1 any mask of admissible orders.  Returns 0, or 2 for a refused mask,
+ * a mask naming an order that does not divide p-1, p < 3 or a failed census.
+ * Every witness run and prefix is certified by direct powers.  cap is
+ * accepted and unused (buffers grow on demand).  One global handle, guarded
+ * by a lock. */
 void baseline_init(unsigned cap);
 int baseline_profile(unsigned p, unsigned mask, unsigned *out, unsigned *prefix, int full);
 

@@ -25,13 +25,18 @@ SRC = HERE / "census_oracle.c"
 
 
 def build(force: bool = False) -> Path:
-    """Compile census_oracle.c into oracle/_build/liboracle.so."""
-    if LIB.exists() and not force and LIB.stat().st_mtime >= SRC.stat().st_mtime:
+    """Compile census_oracle.c into oracle/_build/liboracle.so (rebuilt when
+    the SHA-256 of the source, kept in liboracle.so.key, changes)."""
+    import hashlib
+    key = hashlib.sha256(SRC.read_bytes()).hexdigest()
+    kf = BUILD / "liboracle.so.key"
+    if LIB.exists() and not force and kf.exists() and kf.read_text().strip() == key:
         return LIB
     BUILD.mkdir(exist_ok=True)
     tmp = BUILD / f"liboracle.{os.getpid()}.so"
     subprocess.run(["gcc", "-O2", "-shared", "-fPIC", "-o", str(tmp), str(SRC)], check=True)
     os.replace(tmp, LIB)
+    kf.write_text(key + "\n")
     return LIB
 
 

@@ -48,7 +48,7 @@ EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_coun
            "cz_census", "cz_replay", "cz_a4", "cz_sieve", "cz_plane_bytes", "cz_mem_info", "cz_device_info",
            "cz_microbench", "cz_census_dense_noalloc", "cz_census_interval", "cz_server_open",
            "cz_server_close", "cz_submit", "cz_next_done", "cz_poll", "cz_server_info", "cz_server_last_error",
-           "baseline_init", "baseline_profile"]
+           "cz_prime_count", "baseline_init", "baseline_profile"]
 
 _lib = None
 
@@ -112,6 +112,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.cz_server_info.restype = ctypes.c_int
     L.cz_server_last_error.argtypes = [H]
     L.cz_server_last_error.restype = ctypes.c_char_p
+    L.cz_prime_count.argtypes = [u64, u64]
+    L.cz_prime_count.restype = u64
     L.baseline_init.argtypes = [ctypes.c_uint]
     L.baseline_init.restype = None
     L.baseline_profile.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),

@@ -3,10 +3,14 @@
     python -m rabung_atlas32_b200.build        (or build() from Python)
 
 The library is a plain C-ABI shared object (include/rabung_census.h); the
-Python package loads it with ctypes.
+Python package loads it with ctypes.  A build is reused only when the SHA-256
+of its sources, flags and compiler path (kept beside the library in
+librabung_census.so.key) matches: a library built from other sources, however
+new its file time, is rebuilt.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import subprocess
 import sys
@@ -16,6 +20,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "librabung_census.so"
+KEY = PKG / "librabung_census.so.key"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
@@ -25,9 +30,18 @@ def sources():
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "rabung_census.h"]
 
 
+def source_key(extra=()) -> str:
+    """SHA-256 over every source file's name and bytes, the flags and nvcc."""
+    h = hashlib.sha256()
+    for p in sources():
+        h.update(p.name.encode() + b"\0" + p.read_bytes() + b"\0")
+    h.update(" ".join([NVCC, *FLAGS, *extra]).encode())
+    return h.hexdigest()
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
-    newest = max(p.stat().st_mtime for p in sources())
-    if LIB.exists() and not force and LIB.stat().st_mtime >= newest:
+    key = source_key()
+    if LIB.exists() and not force and KEY.exists() and KEY.read_text().strip() == key:
         return LIB
     tmp = LIB.with_suffix(f".{os.getpid()}.tmp.so")
     cmd = [NVCC, *FLAGS, "-I", str(ROOT / "include"), "-o", str(tmp), str(CSRC / "census.cu")]
@@ -40,6 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if verbose:
         sys.stderr.write(r.stderr)
     os.replace(tmp, LIB)
+    KEY.write_text(key + "\n")
     return LIB
 
 

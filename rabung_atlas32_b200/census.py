@@ -21,6 +21,12 @@ class CensusError(RuntimeError):
     """A refused request: no partial result is returned."""
 
 
+def prime_count(lo: int, hi: int) -> int:
+    """Exact number of primes in [lo, hi), hi <= 2^33, computed on the host by
+    the library (cz_prime_count; needs no GPU)."""
+    return int(_lib.load().cz_prime_count(int(lo), int(hi)))
+
+
 @dataclass
 class Tuning:
     sparse_min_p: int = 1 << 20
@@ -134,8 +140,14 @@ class Census:
         arr = _as_u32_array(primes)
         return int(self.lib.cz_count_profiles(arr, len(primes)))
 
-    def raw(self, primes, mode: str = "auto", a4: bool = True, verify: bool = False):
-        """Run the census; returns (ctypes profile array, A4 list or None, stats dict)."""
+    def raw(self, primes, mode: str = "auto", a4: bool = True, verify: bool = True):
+        """Run the census; returns (ctypes profile array, A4 list or None, stats dict).
+
+        With verify (the default) every witness run is re-proved on the device
+        by direct powers -- monochromatic over its M positions and closed at
+        both ends -- and every dense prefix re-checked, as the reference worker
+        certifies each record before emitting it (src/census/worker32.cu:37-38,
+        B2/src/advance.cpp:7-13); a failure refuses the request."""
         n = len(primes)
         arr = _as_u32_array(primes)
         nprof = int(self.lib.cz_count_profiles(arr, n))
@@ -149,36 +161,30 @@ class Census:
         self.last_stats = st.as_dict()
         return out, (list(a4buf[:n]) if a4 else None), self.last_stats
 
-    def profiles(self, primes, mode: str = "auto", a4: bool = True, verify: bool = False):
+    def profiles(self, primes, mode: str = "auto", a4: bool = True, verify: bool = True):
         """List of codec.Record (profiles ascending r, A4 when requested)."""
         out, a4v, _ = self.raw(primes, mode, a4, verify)
         return to_records(primes, out, a4v)
 
-    def interval(self, lo: int, hi: int, mode: str = "auto", a4: bool = True, max_primes: int = 1 << 20):
+    def interval(self, lo: int, hi: int, mode: str = "auto", a4: bool = True, verify: bool = True,
+                 max_primes: int = 1 << 20):
         """(primes, records) of every prime in [lo, hi): device sieve + census
-        in one library call (cz_census_interval).  Buffers are sized from a
-        prime-count estimate; when it is short, the library reports the
-        exact counts and the call is repeated once with them.  More than
-        max_primes primes in the interval is an error."""
-        import math
+        in one library call (cz_census_interval), its buffers sized from the
+        exact prime count of the interval.  More than max_primes primes in the
+        interval is an error."""
         lo, hi = int(lo), int(hi)
-        est = int((hi - lo) / max(1.0, math.log(max(lo, 3))) * 1.25) + 64
-        cap = max(1, min(int(max_primes), est))
-        out_cap = 8 * cap
-        flags = MODES[mode] | (_lib.CZ_A4 if a4 else 0)
-        for attempt in range(2):
-            ps = (ctypes.c_uint32 * cap)()
-            npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
-            out = (_lib.cz_profile * max(1, out_cap))()
-            a4buf = (ctypes.c_uint32 * cap)() if a4 else None
-            st = _lib.cz_stats()
-            rc = self.lib.cz_census_interval(self.h, lo, hi, flags, ps, cap, ctypes.byref(npr), out, out_cap,
-                                             ctypes.byref(nprof), a4buf, ctypes.byref(st))
-            if rc == _lib.CZ_ELIMIT and attempt == 0 and npr.value <= max_primes:
-                cap = max(1, npr.value)
-                out_cap = max(nprof.value, 8 * cap)
-                continue
-            break
+        cap = prime_count(lo, hi)
+        if cap > max_primes:
+            raise CensusError(f"[{lo}, {hi}) holds {cap} primes, above max_primes = {max_primes}")
+        out_cap = 8 * max(1, cap)
+        flags = MODES[mode] | (_lib.CZ_A4 if a4 else 0) | (_lib.CZ_VERIFY if verify else 0)
+        ps = (ctypes.c_uint32 * max(1, cap))()
+        npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
+        out = (_lib.cz_profile * out_cap)()
+        a4buf = (ctypes.c_uint32 * max(1, cap))() if a4 else None
+        st = _lib.cz_stats()
+        rc = self.lib.cz_census_interval(self.h, lo, hi, flags, ps, max(1, cap), ctypes.byref(npr), out, out_cap,
+                                         ctypes.byref(nprof), a4buf, ctypes.byref(st))
         if rc != 0:
             raise CensusError(f"interval census refused (rc={rc}, primes {npr.value}): {self._err()}")
         self.last_stats = st.as_dict()
@@ -238,12 +244,13 @@ class Census:
             raise CensusError(f"A4 refused (rc={rc}): {self._err()}")
         return list(buf[:n])
 
-    def block(self, lo: int, hi: int, primes=None, mode: str = "auto"):
-        """(scan_frame, a4_frame, records) for the primes of [lo, hi)."""
+    def block(self, lo: int, hi: int, primes=None, mode: str = "auto", verify: bool = True):
+        """(scan_frame, a4_frame, records) for the primes of [lo, hi), every
+        record certified on the device unless verify is False."""
         if primes is None:
             from .sieve import primes_in
             primes = primes_in(lo, hi)
-        recs = self.profiles(primes, mode=mode, a4=True)
+        recs = self.profiles(primes, mode=mode, a4=True, verify=verify)
         return codec.encode_scan_frame(lo, hi, recs), codec.encode_a4_frame(lo, hi, recs), recs
 
 

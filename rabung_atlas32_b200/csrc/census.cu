@@ -84,6 +84,14 @@ bool cover_D(u32 p, u32 B, u32 Q, u32 &Dout) {
 
 u32 popc(u32 x) { return (u32)__builtin_popcount(x); }
 
+// one launch with its own error code: a launch failure is reported through the
+// return value, and an error the caller left pending is neither read nor cleared
+template <class... A>
+bool launch(void (*k)(A...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A... args) {
+    void *argv[] = {static_cast<void *>(&args)...};
+    return cudaLaunchKernel(reinterpret_cast<const void *>(k), grid, block, argv, smem, st) == cudaSuccess;
+}
+
 }  // namespace
 
 struct cz_handle {
@@ -975,15 +983,15 @@ int cz_microbench(cz_handle *h, uint32_t kind, double *per_second) {
 
 // ---- dense census without device allocation ---------------------------------
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-// being captured into a pool it does not own, plugins inside a host process
-// that owns the device's memory budget, or allocator-free embedded services.
-// cz_census_dense_noalloc serves them.  Its only device scratch is the
-// file-scope array below (NOALLOC_BYTES, held by every GPU that loads this
-// library until the process exits); descriptors, run summaries, per-profile
-// state and output records are carved out of it.  The host side uses fixed
-// stack arrays only.  Calls share the array: two calls that overlap on the GPU
-// (different streams, or different host threads) race.
+// Some callers cannot call cudaMalloc: plugins inside a host process that owns
+// the device's memory budget, and allocator-free services that must not grow
+// their device footprint after start-up.  cz_census_dense_noalloc serves them.
+// Its only device scratch is the file-scope array below (NOALLOC_BYTES, held by
+// every GPU that loads this library until the process exits); descriptors, run
+// summaries, per-profile state and output records are carved out of it.  The
+// host side uses fixed stack arrays only.  The call is synchronous: it returns
+// after its stream has finished.  Calls share the array: two calls that overlap
+// on the GPU (different streams, or different host threads) race.
 
 constexpr u32 NOALLOC_BYTES = 2u << 20;          // 2 MiB
 constexpr u32 NOALLOC_MAX_PRIMES = 64;
@@ -1020,23 +1028,18 @@ constexpr NoallocLayout noalloc_layout() {
 }
 static_assert(noalloc_layout().end <= NOALLOC_BYTES, "static scratch too small for its limits");
 
-// device address of the scratch array, resolved once per device with that
-// device current (the host-side name is only a stand-in for the symbol)
-std::mutex g_noalloc_mu;
-unsigned char *g_noalloc_ptr[64] = {};
-
-int noalloc_setup(int dev, unsigned char **out) {
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (dev < 0 || dev >= 64) return CZ_EINVAL;
-    if (!g_noalloc_ptr[dev]) {
-        void *ptr = nullptr;
-        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return CZ_ECUDA;
-        if (cudaFuncSetAttribute(dense_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) !=
-            cudaSuccess)
-            return CZ_ECUDA;
-        g_noalloc_ptr[dev] = static_cast<unsigned char *>(ptr);
-    }
-    *out = g_noalloc_ptr[dev];
+// Set-up for the current device: the device address of the scratch array (the
+// host-side name of the array is only a stand-in for the symbol, never a device
+// address) and the dense kernel's shared-memory limit.  Resolved on every call
+// with the caller's device current, so the address stays right after a
+// cudaDeviceReset reloads the module; both steps are cheap lookups.
+int noalloc_setup(unsigned char **out) {
+    void *ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return CZ_ECUDA;
+    if (cudaFuncSetAttribute(dense_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) !=
+        cudaSuccess)
+        return CZ_ECUDA;
+    *out = static_cast<unsigned char *>(ptr);
     return CZ_OK;
 }
 
@@ -1088,10 +1091,8 @@ extern "C" int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_pr
     }
     if (out_cap < nprof) return CZ_EINVAL;
     if (nprof == 0) return CZ_OK;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return CZ_ECUDA;
     unsigned char *base = nullptr;
-    int rc = noalloc_setup(dev, &base);
+    int rc = noalloc_setup(&base);
     if (rc) return rc;
     constexpr NoallocLayout L = noalloc_layout();
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1106,7 +1107,7 @@ extern "C" int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_pr
     ProfDesc *dD = reinterpret_cast<ProfDesc *>(base + L.profs);
     ProfState *dS = reinterpret_cast<ProfState *>(base + L.state);
     // setup_kernel re-initialises every ProfState this call uses
-    setup_kernel<<<(n + 127) / 128, 128, 0, st>>>(dP, dD, dS, n);
+    if (!launch(setup_kernel, dim3((n + 127) / 128), dim3(128), 0, st, dP, dD, dS, n)) return CZ_ECUDA;
     u32 max_slots = 8;
     for (u32 i = 0; i < n; ++i) max_slots = std::max(max_slots, hash_slots(hp[i].m));
     DenseArgs da;
@@ -1120,7 +1121,9 @@ extern "C" int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_pr
     da.summ = reinterpret_cast<Summ *>(base + L.summ);
     da.state = dS;
     da.seg = DENSE_SEG;
-    dense_scan_kernel<<<std::max(1u, std::min(chunk[nd], 1184u)), DENSE_WARPS * 32, max_slots * 6u + 16u, st>>>(da);
+    if (!launch(dense_scan_kernel, dim3(std::max(1u, std::min(chunk[nd], 1184u))), dim3(DENSE_WARPS * 32),
+                max_slots * 6u + 16u, st, da))
+        return CZ_ECUDA;
     DenseMergeArgs ma;
     ma.primes = dP;
     ma.profs = dD;
@@ -1130,10 +1133,13 @@ extern "C" int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_pr
     ma.summ = da.summ;
     ma.state = dS;
     ma.prefix_out = reinterpret_cast<u32 *>(base + L.dpre);
-    dense_merge_kernel<<<(nprof + 7) / 8, 256, 0, st>>>(ma, reinterpret_cast<u32 *>(base + L.dlist), nprof);
+    const u32 *dl = reinterpret_cast<const u32 *>(base + L.dlist);
+    if (!launch(dense_merge_kernel, dim3((nprof + 7) / 8), dim3(256), 0, st, ma, dl, nprof)) return CZ_ECUDA;
     OutRecord *dO = reinterpret_cast<OutRecord *>(base + L.out);
-    finalize_kernel<<<(nprof + 127) / 128, 128, 0, st>>>(dP, dD, dS, ma.prefix_out, nprof, 0u, dO);
-    if (cudaGetLastError() != cudaSuccess) return CZ_ECUDA;
+    const u32 *dpre = ma.prefix_out;
+    if (!launch(finalize_kernel, dim3((nprof + 127) / 128), dim3(128), 0, st, (const PrimeDesc *)dP,
+                (const ProfDesc *)dD, (const ProfState *)dS, dpre, nprof, 0u, dO))
+        return CZ_ECUDA;
     static_assert(sizeof(OutRecord) == sizeof(cz_profile), "record layout");
     if (cudaMemcpyAsync(out, dO, sizeof(OutRecord) * nprof, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return CZ_ECUDA;
@@ -1144,25 +1150,104 @@ extern "C" int cz_census_dense_noalloc(const uint32_t *primes, uint32_t n, cz_pr
 }
 
 // ---- reference-compatible adapter -------------------------------------------
+//
+// The reference's only in-process C ABI (src/census/engine32/src/baseline_bridge.cu:7,21-27):
+// with full = 0 it serves exactly the order sets {2}, {2,4}, {3,6}, {2,3,6} and
+// {2,3,4,6} (masks 1, 5, 18, 19, 23) and returns 2 for any other mask; with
+// full = 1 it profiles every admissible order and reports those in the mask.
+// Here the same rule holds, and a mask naming an order that does not divide
+// p - 1 is refused with 2 as well (the reference reads an undefined colouring
+// there).  cap (the reference's largest p, which sizes its buffers) is not
+// needed: the handle grows its buffers on demand.
 static cz_handle *g_base = nullptr;
+static std::mutex g_base_mu;
 
 void baseline_init(unsigned cap) {
     (void)cap;
+    std::lock_guard<std::mutex> lk(g_base_mu);
     if (!g_base) cz_open(nullptr, &g_base);
 }
 
 int baseline_profile(unsigned p, unsigned mask, unsigned *out, unsigned *prefix, int full) {
-    (void)full;
-    if (!g_base) baseline_init(0);
-    if (!g_base || p < 3u) return 2;
+    if (!full && mask != 1u && mask != 5u && mask != 18u && mask != 19u && mask != 23u) return 2;
+    if (!out || !prefix || p < 3u) return 2;
     const u32 adm = mask_of(p);
     if (mask & ~adm) return 2;
+    baseline_init(0);
+    std::lock_guard<std::mutex> lk(g_base_mu);
+    if (!g_base) return 2;
     std::vector<cz_profile> rec(popc(adm));
     u32 pp = p;
-    if (cz_census(g_base, &pp, 1, CZ_AUTO, rec.data(), (u32)rec.size(), nullptr, nullptr)) return 2;
+    if (cz_census(g_base, &pp, 1, CZ_AUTO | CZ_VERIFY, rec.data(), (u32)rec.size(), nullptr, nullptr)) return 2;
     for (const cz_profile &v : rec)
         if (mask & (1u << (v.r - 2))) { out[v.r] = v.M; prefix[v.r] = v.L; }
     return 0;
+}
+
+// ---- exact prime counts on the host -----------------------------------------
+//
+// pi(x) by the Lucy-Hedgehog recursion over the values floor(x / k): S(v)
+// starts at v - 1 and, for each prime q <= sqrt(x) in turn, every v >= q^2
+// loses S(v / q) - S(q - 1) (the integers whose least prime factor is q);
+// O(x^(3/4)) time, O(sqrt x) memory -- a few ms at x = 2^32.  It plays the
+// role of the reference's Meissel-Lehmer count (src/census/prime_count.cpp:11-24):
+// interval buffers are sized exactly in one pass, without sieving ahead.
+// Short intervals are counted by a segmented sieve instead.
+
+namespace {
+
+u64 isqrt64(u64 x) {
+    u64 r = (u64)std::sqrt((double)x);
+    while (r * r > x) --r;
+    while ((r + 1) * (r + 1) <= x) ++r;
+    return r;
+}
+
+u64 lucy_pi(u64 x) {
+    if (x < 2) return 0;
+    const u64 r = isqrt64(x);
+    std::vector<u64> lo(r + 1), hi(r + 1);     // lo[v] = S(v), hi[k] = S(x / k)
+    for (u64 v = 1; v <= r; ++v) lo[v] = v - 1;
+    for (u64 k = 1; k <= r; ++k) hi[k] = x / k - 1;
+    for (u64 q = 2; q <= r; ++q) {
+        if (lo[q] == lo[q - 1]) continue;          // q composite
+        const u64 sp = lo[q - 1], q2 = q * q;
+        const u64 kmax = std::min(r, x / q2);
+        for (u64 k = 1; k <= kmax; ++k) {
+            const u64 kq = k * q;
+            const u64 sub = kq <= r ? hi[kq] : lo[x / kq];
+            hi[k] -= sub - sp;
+        }
+        for (u64 v = r; v >= q2; --v) lo[v] -= lo[v / q] - sp;
+    }
+    return hi[1];
+}
+
+// primes in [lo, hi) by a segmented sieve (hi - lo small)
+u64 sieve_count(u64 lo, u64 hi) {
+    if (hi <= 2) return 0;
+    if (lo < 2) lo = 2;
+    if (lo >= hi) return 0;
+    const u64 r = isqrt64(hi - 1);
+    std::vector<char> small(r + 1, 1), seg(hi - lo, 1);
+    for (u64 q = 2; q <= r; ++q) {
+        if (!small[q]) continue;
+        for (u64 j = q * q; j <= r; j += q) small[j] = 0;
+        u64 s = std::max(q * q, (lo + q - 1) / q * q);
+        for (u64 j = s; j < hi; j += q) seg[j - lo] = 0;
+    }
+    u64 c = 0;
+    for (char v : seg) c += (u64)v;
+    return c;
+}
+
+}  // namespace
+
+uint64_t cz_prime_count(uint64_t lo, uint64_t hi) {
+    if (hi > (1ull << 33)) hi = 1ull << 33;
+    if (lo >= hi) return 0;
+    if (hi - lo <= (1ull << 22)) return sieve_count(lo, hi);
+    return lucy_pi(hi - 1) - (lo >= 2 ? lucy_pi(lo - 1) : 0);
 }
 
 }  // extern "C"

@@ -170,39 +170,29 @@ int cz_census_interval(cz_handle *h, uint64_t lo, uint64_t hi, uint32_t flags, u
     if (!h || !n_primes || !n_profiles || lo > hi || hi > (1ull << 32)) return CZ_EINVAL;
     *n_primes = 0;
     *n_profiles = 0;
+    // exact prime count first: a short buffer is reported with the needed
+    // count before any device work
+    const uint64_t count = cz_prime_count(lo, hi);
+    if (count > primes_cap) {
+        *n_primes = (uint32_t)std::min<uint64_t>(0xFFFFFFFFull, count);
+        return CZ_ELIMIT;
+    }
     std::vector<uint32_t> ps;
+    ps.reserve(count);
     uint64_t cur = std::max<uint64_t>(lo, 2);
-    while (cur < hi) {
-        // one more than the room left, to see past hi or past the capacity
-        const uint32_t want = (uint32_t)std::min<uint64_t>((uint64_t)primes_cap - ps.size() + 1u, 32768u);
+    while (cur < hi && ps.size() < count) {
+        const uint32_t want = (uint32_t)std::min<uint64_t>(count - ps.size(), 32768u);
         std::vector<uint32_t> got(want);
         uint32_t found = 0, clo = (uint32_t)cur;
         const int rc = cz_sieve(h, &clo, &want, 1, got.data(), &found);
         if (rc) return rc;
-        bool end = found < want;
-        for (uint32_t i = 0; i < found; ++i) {
-            if (got[i] >= hi) { end = true; break; }
-            ps.push_back(got[i]);
-        }
-        if (ps.size() > primes_cap) break;
-        if (end || found == 0) break;
+        for (uint32_t i = 0; i < found && got[i] < hi; ++i) ps.push_back(got[i]);
+        if (found < want || found == 0) break;
         cur = (uint64_t)got[found - 1] + 1u;
     }
-    if (ps.size() > primes_cap) {             // count the rest so the caller can size its buffers
-        uint64_t extra = 0;
-        uint64_t c2 = (uint64_t)ps.back() + 1u;
-        while (c2 < hi) {
-            const uint32_t want = 32768u;
-            std::vector<uint32_t> got(want);
-            uint32_t found = 0, clo = (uint32_t)c2;
-            if (cz_sieve(h, &clo, &want, 1, got.data(), &found)) break;
-            uint32_t i = 0;
-            for (; i < found && got[i] < hi; ++i) ++extra;
-            if (i < found || found < want) break;
-            c2 = (uint64_t)got[found - 1] + 1u;
-        }
-        *n_primes = (uint32_t)std::min<uint64_t>(0xFFFFFFFFull, ps.size() + extra);
-        return CZ_ELIMIT;
+    if (ps.size() != count) {
+        h->err = "device sieve and prime count disagree on [" + std::to_string(lo) + ", " + std::to_string(hi) + ")";
+        return CZ_EREFUSED;
     }
     *n_primes = (uint32_t)ps.size();
     if (!ps.empty() && !primes_out) return CZ_EINVAL;

@@ -487,7 +487,7 @@ def run(atlas: Atlas, census, lo: int, hi: int, block_primes: int = BLOCK_PRIMES
         ps, bhi = next_block_primes(census, cur, hi, block_primes)
         if not ps:                       # no prime left in [cur, hi): nothing to record
             break
-        recs = census.profiles(ps, mode=mode, a4=True)
+        recs = census.profiles(ps, mode=mode, a4=True, verify=True)
         bid = atlas.next_block
         audits = []
         if audit_every and bid % audit_every == 0:

@@ -110,7 +110,7 @@ class Server:
     def submit(self, lo: int, count: int, flags: int | None = None) -> int:
         ct = self._ct
         rid = ct.c_uint64()
-        fl = (self._L.CZ_AUTO | self._L.CZ_A4) if flags is None else flags
+        fl = (self._L.CZ_AUTO | self._L.CZ_A4 | self._L.CZ_VERIFY) if flags is None else flags
         rc = self.lib.cz_submit(self.h, int(lo), int(count), None, fl, ct.byref(rid))
         if rc != 0:
             raise RuntimeError(f"cz_submit failed (rc={rc})")

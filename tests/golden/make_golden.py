@@ -4,7 +4,7 @@
 Run once in a container that has the reference mounted, after
 `make -f oracle/Makefile.ref REF=<reference>`:
 
-    python tests/golden/make_golden.py --ref /root/reference
+    python tests/golden/make_golden.py --ref <reference checkout>
 
 Writes into tests/golden/:
   scan-00000.vdw, quadruplets-00000.a4, scan-49900.vdw, quadruplets-49900.a4,
@@ -19,9 +19,12 @@ Writes into tests/golden/:
                         and throughput/CONTROLES_INDEPENDANTS.json (p < 2^32).
   refcpu_top_block.json.gz -- outputs of the reference's own CPU programs
                         (oracle/_ref) on the 4096 primes ending at 4294967291:
-                        moment_worker A4 for all of them and the sparse CPU
-                        engine `advance adaptive p r 64 3 1` on a seeded
-                        sample of (p, r) pairs below block 49900.
+                        moment_worker A4 for all of them and, for EVERY
+                        admissible (p, r) of the 1783 primes below block 49900
+                        (block 49900's own frame pins the other 2313), the
+                        reference's sparse CPU engines: `target p c f 64 1 8192 1`
+                        for the coupled pairs {2, 4} and {3, 6}, `advance
+                        adaptive p r 64 3 1` for every other order.
   refcpu_2p24.json.gz -- `independent p r 3` (full-walk reference) on a seeded
                         sample of (p, r) pairs from the 4096 primes from 2^24,
                         and moment_worker A4 for all 4096 of them.
@@ -46,8 +49,9 @@ import oracle  # noqa: E402  (checker, used here only to list primes)
 
 
 def dump(name, obj):
-    with gzip.open(HERE / name, "wt") as f:
-        json.dump(obj, f, separators=(",", ":"))
+    """gzip'd compact JSON, byte-reproducible (no timestamp in the header)."""
+    raw = json.dumps(obj, separators=(",", ":")).encode()
+    (HERE / name).write_bytes(gzip.compress(raw, mtime=0))
 
 
 def consecutive_primes_from(start, n):
@@ -85,8 +89,9 @@ def moment_worker(ref_bin, primes):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--samples", type=int, default=48)
+    ap.add_argument("--ref", required=True, help="checkout of the reference repository")
+    ap.add_argument("--samples", type=int, default=48, help="(p, r) pairs of the 2^24 block for `independent`")
+    ap.add_argument("--jobs", type=int, default=8)
     a = ap.parse_args()
     ref = Path(a.ref)
     ref_bin = REPO / "oracle" / "_ref"
@@ -121,22 +126,35 @@ def main():
     top = consecutive_primes_ending(4294967291, 4096)
     a4_top = moment_worker(ref_bin, top)
     below = [p for p in top if p < 4294915433]
-    pairs = []
-    while len(pairs) < a.samples:
-        p = rng.choice(below)
+    jobs = []
+    for p in below:
         rs = [r for r in range(2, 10) if (p - 1) % r == 0]
-        pairs.append((p, rng.choice(rs)))
+        for c, f in ((2, 4), (3, 6)):
+            if c in rs and f in rs:
+                jobs.append(("target", p, c, f))
+                rs = [r for r in rs if r not in (c, f)]
+        jobs += [("advance", p, r, 0) for r in rs]
 
-    def run_adv(pr):
-        p, r = pr
+    def run_job(job):
+        kind, p, r, f = job
+        if kind == "target":
+            out = subprocess.run([str(ref_bin / "target"), str(p), str(r), str(f), "64", "1", "8192", "1"],
+                                 capture_output=True, check=True, text=True).stdout
+            j = json.loads(out)
+            assert j["status"] == "PASS", (p, r, f)
+            return [[p, r, j["coarse_maximum"], j["coarse_prefix"], j["coarse_witness"]],
+                    [p, f, j["fine_maximum"], j["fine_prefix"], j["fine_witness"]]]
         out = subprocess.run([str(ref_bin / "advance"), "adaptive", str(p), str(r), "64", "3", "1"],
                              capture_output=True, check=True, text=True).stdout
         j = json.loads(out)
-        return [p, r, j["maximum"], j["prefix"], j["witness"]]
+        assert j["status"] == "PASS", (p, r)
+        return [[p, r, j["maximum"], j["prefix"], j["witness"]]]
 
-    with ThreadPoolExecutor(8) as ex:
-        adv = list(ex.map(run_adv, pairs))
-    dump("refcpu_top_block.json.gz", {"primes": top, "a4": a4_top, "advance": adv})
+    with ThreadPoolExecutor(a.jobs) as ex:
+        res = list(ex.map(run_job, jobs))
+    adv = sorted(v for part, job in zip(res, jobs) if job[0] == "advance" for v in part)
+    tgt = sorted(v for part, job in zip(res, jobs) if job[0] == "target" for v in part)
+    dump("refcpu_top_block.json.gz", {"primes": top, "a4": a4_top, "advance": adv, "target": tgt})
 
     # 2^24 block
     low = consecutive_primes_from(2 ** 24, 4096)

@@ -196,3 +196,43 @@ def test_refusal_leaves_no_stale_state(eng):
     small = sieve.primes_in(3, 500)
     got = eng.profiles(small, mode="auto", a4=True)
     assert [r.a4 for r in got] == [oracle.a4(p) for p in small]
+
+
+def test_reference_c_abi_baseline_profile(golden):
+    """The reference's own in-process C ABI (baseline_init / baseline_profile,
+    src/census/engine32/src/baseline_bridge.cu:7,21-27), called through ctypes
+    as a reference maintainer would bind it: M into out[r] and L into
+    prefix[r] equal block 49900's records; with full = 0 only the masks
+    1, 5, 18, 19, 23 are served and any other returns 2, as there."""
+    import ctypes
+    from rabung_atlas32_b200 import _lib
+    lib = _lib.load()
+    lib.baseline_init(0xFFFFFFFF)
+    recs, _, _ = golden["49900"]
+    rng = random.Random(20261203)
+    served = {1: {2}, 5: {2, 4}, 18: {3, 6}, 19: {2, 3, 6}, 23: {2, 3, 4, 6}}
+    checked = 0
+    for rec in rng.sample(recs, 40):
+        adm = {v.r for v in rec.profiles}
+        mask_all = sum(1 << (r - 2) for r in adm)
+        by = {v.r: (v.M, v.L) for v in rec.profiles}
+        out = (ctypes.c_uint * 10)()
+        pre = (ctypes.c_uint * 10)()
+        assert lib.baseline_profile(rec.p, mask_all, out, pre, 1) == 0
+        for r in adm:
+            assert (out[r], pre[r]) == by[r], (rec.p, r)
+            checked += 1
+        for mask, rs in served.items():
+            out2 = (ctypes.c_uint * 10)()
+            pre2 = (ctypes.c_uint * 10)()
+            rc = lib.baseline_profile(rec.p, mask, out2, pre2, 0)
+            if rs <= adm:
+                assert rc == 0
+                assert all((out2[r], pre2[r]) == by[r] for r in rs), (rec.p, mask)
+            else:
+                assert rc == 2, (rec.p, mask)
+        # a mask outside the five without `full` is refused even when admissible
+        if {2, 3} <= adm:
+            assert lib.baseline_profile(rec.p, 0b11, out, pre, 0) == 2
+            assert lib.baseline_profile(rec.p, 0b11, out, pre, 1) == 0
+    assert checked > 100

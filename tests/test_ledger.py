@@ -157,14 +157,16 @@ class FakeCensus:
         self.recs = {r.p: r for r in blocks["00000"][0]}
         self.planted = planted
         self.calls = []
+        self.verify_flags = []
 
     def sieve(self, requests):
         from rabung_atlas32_b200 import sieve
         return [sieve.primes_from(lo, n) for lo, n in requests]
 
-    def profiles(self, primes, mode="auto", a4=True):
+    def profiles(self, primes, mode="auto", a4=True, verify=False):
         import copy
         self.calls.append(mode)
+        self.verify_flags.append((mode, verify))
         out = [copy.deepcopy(self.recs[p]) for p in primes]
         for r in out:
             if mode == "dense" and r.p == self.planted:
@@ -187,6 +189,8 @@ def test_supervisor_cuts_blocks_resumes_and_audits(tmp_path, blocks):
         assert res["primes"] == 4096 and res["GPU_audits"] == res["A4_certificate_audits"] == 3
         got = [r.p for b in range(5) for r in codec.decode_scan_frame(at.frame("scan", b))[0]]
         assert got == [r.p for r in blocks["00000"][0]]
+    # every committed block's records were certified on the device
+    assert all(v for m, v in fake.verify_flags if m != "dense")
     # a whole-block run reproduces the sample frames
     with ledger.Atlas(tmp_path / "one") as at:
         ledger.run(at, FakeCensus(blocks), 1, 38891, audit_every=1, log=lambda s: None)

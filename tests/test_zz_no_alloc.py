@@ -1,9 +1,9 @@
 """The allocation-free dense census entry point (cz_census_dense_noalloc).
 
-It exists for callers that cannot call cudaMalloc (code inside a CUDA graph
-capture into a pool it does not own, plugins in a host process that owns the
-device memory budget, allocator-free services): its only device scratch is a
-fixed 2 MiB array inside the library.  This file is collected last so that a
+It exists for callers that cannot call cudaMalloc (plugins in a host process
+that owns the device memory budget, allocator-free services that must not grow
+their device footprint after start-up): its only device scratch is a fixed
+2 MiB array inside the library, and the call is synchronous.  This file is collected last so that a
 run stopping at the first failure has already run every other test.  The
 records must equal those of the regular entry point (cz_census, dense mode)
 exactly -- integer results, zero tolerance -- on two calls in a row (the

@@ -97,19 +97,28 @@ def test_2p24_block_dense_vs_reference_and_sparse(eng):
 
 
 def test_top_block_sparse_vs_reference_cpu(eng, golden):
-    """C3: 4096 primes ending at 4294967291: A4 vs moment_worker for all; the
-    reference sparse CPU engine on a seeded sample below block 49900; block
-    49900's own records for the rest."""
+    """C3, all 13,660 profiles: 4096 primes ending at 4294967291 by the anchor
+    filter, every record certified on the device.  The 1783 primes below
+    block 49900 (5914 profiles) against the reference's own CPU sparse engines
+    run on every one of their (p, r) pairs -- `target` for the coupled pairs
+    {2, 4} and {3, 6}, `advance` for the other orders -- and the 2313 primes of
+    block 49900 against its shipped frame; A4 against moment_worker for all."""
     d = load_gz("refcpu_top_block.json.gz")
     ps = d["primes"]
-    got = eng.profiles(ps, mode="sparse", a4=True)
+    got = eng.profiles(ps, mode="sparse", a4=True, verify=True)
     assert [r.a4 for r in got] == d["a4"]
-    by = {(r.p, v.r): (v.M, v.L, v.witness) for r in got for v in r.profiles}
-    for p, r, M, L, w in d["advance"]:
-        assert by[(p, r)] == (M, L, w)
+    ref = {(p, r): (M, L, w) for p, r, M, L, w in d["advance"] + d["target"]}
     recs, _, _ = golden["49900"]
     top = {r.p: r for r in got}
+    lower = [r for r in got if r.p < recs[0].p]
+    n = 0
+    for rec in lower:
+        for v in rec.profiles:
+            assert ref[(rec.p, v.r)] == (v.M, v.L, v.witness), (rec.p, v.r)
+            n += 1
+    assert n == len(ref) == 5914
     assert tup([top[r.p] for r in recs]) == golden_tup(recs)
+    assert n + sum(len(r.profiles) for r in recs) == 13660
 
 
 def test_top_block_dense_judge_1pct(eng):

@@ -47,6 +47,7 @@ import zlib
 from pathlib import Path
 
 from . import codec
+from .census import prime_count
 
 PACK_BYTES = 64 << 20          # a new pack file starts past this size
 BLOCK_PRIMES = 4096            # primes per block (the frame maximum)
@@ -319,6 +320,10 @@ class Atlas:
             if self.contiguous:
                 check(s[0] == prev_id + 1 and s[1] == lo_expect, f"block {s[0]}: not contiguous")
             check(s[1] >= lo_expect, f"block {s[0]}: overlaps its predecessor")
+            # the block holds every prime of its interval: its count equals the
+            # exact host count pi(hi - 1) - pi(lo - 1)
+            check(prime_count(s[1], s[2]) == s[3], f"block {s[0]}: {s[3]} primes, [lo, hi) holds "
+                                                  f"{prime_count(s[1], s[2])}")
             for sub, row in (("scan", s), ("quadruplets", a)):
                 key = f"{sub}/{row[4]}"
                 check(row[5] == offsets.get(key, 0) and row[6] > 0, f"block {s[0]}: {key} extent not contiguous")
@@ -355,6 +360,8 @@ class Atlas:
             check(int(meta["next_lo"]) == lo_expect and int(meta["next_block"]) == prev_id + 1, "next_lo / next_block")
             check(int(meta["prime_count"]) == primes, "prime_count")
         check(int(am["sum_A4"]) == total_a4, "sum_A4")
+        if self.contiguous:
+            check(primes == prime_count(1, lo_expect), "prime_count differs from pi(next_lo - 1)")
         check(int(m["profile_count"]) == profiles, "profile_count")
         calc = {name: {r: dict(c) for r, c in orders.items()} for name, orders in agg.items()}
         stored = json.loads(m["aggregate"])

@@ -208,3 +208,18 @@ def test_supervisor_stops_before_committing_a_failed_audit(tmp_path, blocks):
         assert at.next_lo == 1 and at.next_block == 0
     with ledger.Atlas(tmp_path) as at:
         assert at.recovered == [] and at.verify()["blocks"] == 0
+
+
+def test_verify_catches_a_block_missing_a_prime(tmp_path, blocks):
+    """A sieve that silently drops a prime yields a block whose count is short
+    of the exact prime count of its interval; verify() refuses the atlas."""
+    class DroppingCensus(FakeCensus):
+        def sieve(self, requests):
+            out = super().sieve(requests)
+            return [[p for p in ps if p != 1009] for ps in out]
+
+    with ledger.Atlas(tmp_path) as at:
+        ledger.run(at, DroppingCensus(blocks), 1, 38891, block_primes=1000, audit_every=0, max_blocks=1,
+                   log=lambda s: None)
+        with pytest.raises(ledger.LedgerError, match="primes, \\[lo, hi\\) holds"):
+            at.verify()

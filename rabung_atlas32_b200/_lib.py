@@ -26,7 +26,7 @@ class cz_profile(ctypes.Structure):
 class cz_config(ctypes.Structure):
     _fields_ = [("device", i32), ("sparse_min_p", u32), ("cover_n", u32), ("q_cap", u32 * 10),
                 ("anchor_bits", u32), ("screen", u32), ("sparse_blocks", u32), ("use_graph", u32),
-                ("cta_per_profile", u32), ("l1_carveout", u32), ("speculate", u32),
+                ("cta_per_profile", u32), ("epoch_rows", u32), ("speculate", u32),
                 ("spec_margin10", u32 * 10), ("plane_budget_mb", u32), ("dense_steps", u32),
                 ("anchor_t", u32 * 10), ("reserved", u32 * 1)]
 

@@ -6,7 +6,8 @@ Searches, by coordinate descent from the defaults, the knobs that set how the
 work is cut and scheduled:
   * anchor filter: anchor length policy (anchor_bits, then stages per order
     r, anchor_t), cover window cap and speculation margin per order r, CTAs per profile
-    (cta_per_profile: warps sharing one profile's row queue), L1 carveout,
+    (cta_per_profile: CTAs sharing one profile's work items), rows per
+    threshold epoch (epoch_rows),
     cover shape (cover_n: table radius vs rows), on a sample of the block below
     2^32;
   * dense scan: segment length (dense_steps, x per warp task), on primes near
@@ -81,7 +82,7 @@ def tune(quick: bool = False, log=print) -> dict:
     log(f"baseline sparse {ref_ms:.1f} ms")
     best = dataclasses.replace(base)
     best_ms = ref_ms
-    space = {"anchor_bits": [3, 4, 5], "cta_per_profile": [1, 2, 3, 4], "l1_carveout": [10, 20, 30, 101],
+    space = {"anchor_bits": [3, 4, 5], "cta_per_profile": [1, 2, 3, 4], "epoch_rows": [128, 256, 512],
              "cover_n": [3, 4]}
     rejected = []
     for _ in range(1 if quick else 2):

@@ -37,7 +37,7 @@ class Tuning:
     sparse_blocks: int = 0
     use_graph: int = 1
     cta_per_profile: int = 2
-    l1_carveout: int = 20
+    epoch_rows: int = 256
     speculate: int = 1
     spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 10, 0, 5, 10)
     plane_budget_mb: int = 24 * 1024
@@ -100,7 +100,7 @@ class Census:
         cfg.sparse_blocks = t.sparse_blocks
         cfg.use_graph = t.use_graph
         cfg.cta_per_profile = t.cta_per_profile
-        cfg.l1_carveout = t.l1_carveout
+        cfg.epoch_rows = t.epoch_rows
         cfg.speculate = t.speculate
         for r in range(10):
             cfg.spec_margin10[r] = t.spec_margin10[r]

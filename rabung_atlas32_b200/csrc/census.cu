@@ -9,9 +9,8 @@
 //   finalize_kernel: prefix, optional direct certification, K, records;
 //   a4_kernel: quadratic A4 counts.
 // The device work of the last call can be replayed on resident inputs
-// (cz_replay), optionally through a captured CUDA graph.  The plane pool is
-// also bound to linear textures (one per 512 MiB chunk and texel format) for
-// the filter's texture-pipe loads.  runtime.cuh, included at the end, adds the
+// (cz_replay), optionally through a captured CUDA graph.  runtime.cuh,
+// included at the end, adds the
 // interval census and the serving runtime on top of these entry points.
 #include <algorithm>
 #include <cmath>
@@ -121,11 +120,6 @@ struct cz_handle {
     std::vector<OutRecord> hout;
     void *pin = nullptr;
     size_t pin_cap = 0;
-    Buf b_tex;                               // texture handles [texel format][pool chunk]
-    std::vector<cudaTextureObject_t> tex;
-    void *tex_for = nullptr;
-    size_t tex_cap = 0;
-    u32 tex_chunks = 0;
 };
 
 namespace {
@@ -245,10 +239,12 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
         P.route = sparse ? 2u : 1u;
         if (sparse) {
             P.B = B;
+            // view widths in words, multiples of 4: every view and every tile
+            // copy of the filter starts on a 16-byte boundary
             P.K0 = (B + 31u) / 32u + 4u;
-            P.nwords = 2u * P.K0 + 8u;
+            P.nwords = (2u * P.K0 + 8u + 3u) & ~3u;
             P.K2 = (B + 63u) / 64u + 4u;
-            P.nwords2 = 2u * P.K2 + 8u;
+            P.nwords2 = (2u * P.K2 + 8u + 3u) & ~3u;
             h->h_sidx.push_back(i);
             max_slots_t = std::max(max_slots_t, hash_slots(P.m));
         } else {
@@ -277,10 +273,7 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
                 D.qspec = qspec_for(c, p, r, !(flags & CZ_NOSPEC));
                 D.tpref = c.anchor_t[r] ? c.anchor_t[r] : anchor_pref(r, c.anchor_bits);
                 const u64 pw = ((u64)D.npp * (P.nwords + P.nwords2) + 7ull) & ~7ull;
-                // no profile block straddles a texture chunk of the pool
-                if ((plane_words >> TEX_CHUNK_WORDS_LOG2) != ((plane_words + pw - 1ull) >> TEX_CHUNK_WORDS_LOG2))
-                    plane_words = ((plane_words >> TEX_CHUNK_WORDS_LOG2) + 1ull) << TEX_CHUNK_WORDS_LOG2;
-                D.plane_off = plane_words;              // multiple of 8 words: vector loads and texels align
+                D.plane_off = plane_words;              // multiple of 8 words: vector loads and tile copies align
                 plane_words += pw;
                 D.local = (u32)h->h_sidx.size() - 1u;
                 h->h_slist.push_back((u32)h->hprof.size());
@@ -349,38 +342,6 @@ int plan(cz_handle *h, const u32 *primes, u32 n, u32 flags) {
         !ensure(h, h->b_a4, 4ull * n) ||
         !ensure(h, h->b_counter, 64))
         return CZ_ECUDA;
-    // linear textures over the plane pool, one per chunk and texel format
-    // (uint, uint2, uint4 for 1, 2, 4 stored planes; a 512 MiB chunk holds at
-    // most 2^27 texels, within the 1-D linear texture limit), rebuilt when the
-    // pool moves; the filter fetches the windows of the plane counts in
-    // CZ_TEX_MASK through them
-    if (h->tex_for != h->b_planes.p || h->tex_cap != h->b_planes.cap) {
-        for (auto t : h->tex) cudaDestroyTextureObject(t);
-        h->tex.clear();
-        const size_t chunk = (size_t)4 << TEX_CHUNK_WORDS_LOG2;
-        const size_t nch = (h->b_planes.cap + chunk - 1) / chunk;
-        const cudaChannelFormatDesc fmt[3] = {cudaCreateChannelDesc<unsigned int>(), cudaCreateChannelDesc<uint2>(),
-                                              cudaCreateChannelDesc<uint4>()};
-        for (int f = 0; f < 3; ++f)
-            for (size_t k = 0; k < nch; ++k) {
-                const size_t off = k * chunk;
-                cudaResourceDesc rd{};
-                rd.resType = cudaResourceTypeLinear;
-                rd.res.linear.devPtr = (char *)h->b_planes.p + off;
-                rd.res.linear.desc = fmt[f];
-                rd.res.linear.sizeInBytes = std::min(chunk, h->b_planes.cap - off) & ~(size_t)15;
-                cudaTextureDesc td{};
-                td.readMode = cudaReadModeElementType;
-                cudaTextureObject_t t = 0;
-                if (!ck(h, cudaCreateTextureObject(&t, &rd, &td, nullptr), "texture")) return CZ_ECUDA;
-                h->tex.push_back(t);
-            }
-        h->tex_chunks = (u32)nch;
-        if (!ensure(h, h->b_tex, 8ull * h->tex.size())) return CZ_ECUDA;
-        cudaMemcpy(h->b_tex.p, h->tex.data(), 8ull * h->tex.size(), cudaMemcpyHostToDevice);
-        h->tex_for = h->b_planes.p;
-        h->tex_cap = h->b_planes.cap;
-    }
     h->flags = flags;
     h->have_plan = true;
     return CZ_OK;
@@ -464,10 +425,9 @@ int enqueue(cz_handle *h, bool timed, u32 &launches) {
         // (up to 64), so small calls fill the GPU; large calls keep the tuned group
         sa.group = std::max(std::max(1u, h->cfg.cta_per_profile), std::min(64u, grid / std::max(1u, h->nsl)));
         sa.tune.screen = h->cfg.screen;
-        sa.texs = P<unsigned long long>(h->b_tex);
-        sa.tex_chunks = h->tex_chunks;
+        sa.epoch_rows = h->cfg.epoch_rows;
         grid = std::min(grid, h->nsl * sa.group);
-        sparse_kernel<<<grid, SPARSE_WARPS * 32, 0, st>>>(sa);
+        sparse_kernel<<<grid, SPARSE_WARPS * 32, TILE_WORDS * 4u, st>>>(sa);
         ++launches;
     }
     rec(3);
@@ -566,7 +526,7 @@ int cz_default_config(cz_config *c) {
     c->sparse_blocks = 0;
     c->use_graph = 1;
     c->cta_per_profile = 2;
-    c->l1_carveout = 20;
+    c->epoch_rows = EPOCH_ROWS_DEFAULT;
     c->speculate = 1;
     c->plane_budget_mb = 24u * 1024u;
     c->dense_steps = DENSE_STEPS;
@@ -587,6 +547,7 @@ int cz_open(const cz_config *cfg, cz_handle **out) {
         if (h->cfg.q_cap[r] && (h->cfg.q_cap[r] < 3 || h->cfg.q_cap[r] > 255)) { delete h; return CZ_EINVAL; }
     for (int r = 0; r < 10; ++r)
         if (h->cfg.anchor_t[r] && (h->cfg.anchor_t[r] < 2 || h->cfg.anchor_t[r] > 32)) { delete h; return CZ_EINVAL; }
+    if (h->cfg.epoch_rows > (1u << 20)) { delete h; return CZ_EINVAL; }
     h->dev = h->cfg.device;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || h->dev < 0 || h->dev >= ndev) { delete h; return CZ_ECUDA; }
@@ -599,10 +560,10 @@ int cz_open(const cz_config *cfg, cz_handle **out) {
     cudaFuncSetAttribute(table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_DYN_SMEM);
     cudaFuncSetAttribute(dense_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     cudaFuncSetAttribute(sieve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SIEVE_MAX_WIDTH / 16 + 64);
-    // the filter needs ~20 KB of shared memory per CTA: give the rest of the
-    // unified L1/shared array to L1, where the colour planes are cached
-    if (h->cfg.l1_carveout <= 100)
-        cudaFuncSetAttribute(sparse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)h->cfg.l1_carveout);
+    // the filter stages its tiles in shared memory: the whole unified array
+    // goes to shared memory, two CTAs of TILE_WORDS words each per SM
+    cudaFuncSetAttribute(sparse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TILE_WORDS * 4u));
+    cudaFuncSetAttribute(sparse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (!build_static_tables(h)) { cz_close(h); return CZ_ECUDA; }
     *out = h;
     return CZ_OK;
@@ -616,8 +577,6 @@ void cz_close(cz_handle *h) {
     Buf *bufs[] = {&h->b_in, &h->b_primes, &h->b_profs, &h->b_state, &h->b_planes, &h->b_summ, &h->b_chunk,
                    &h->b_summp, &h->b_didx, &h->b_sidx, &h->b_slist, &h->b_dlist, &h->b_dpre, &h->b_out,
                    &h->b_a4, &h->b_counter, &h->b_sreq, &h->b_sout};
-    for (auto t : h->tex) cudaDestroyTextureObject(t);
-    if (h->b_tex.p) cudaFree(h->b_tex.p);
     for (Buf *b : bufs) if (b->p) cudaFree(b->p);
     if (h->pin) cudaFreeHost(h->pin);
     if (h->d_small) cudaFree(h->d_small);

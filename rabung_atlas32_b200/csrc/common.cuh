@@ -148,10 +148,11 @@ struct ProfDesc {
 // device-written per-profile results
 struct ProfState {
     unsigned long long best;  // packed key of the best completed run
+    unsigned long long claim; // sparse filter: next work item, current epoch and its threshold
     u32 seed;                 // longest monochromatic stretch seen in [1, B]
     u32 firstnz;              // least n >= 1 with colour != 0 (prefix + 1)
-    u32 rows_next;            // rows d handed out (sparse filter)
     u32 status;
+    u32 pad;
     unsigned long long words;       // filter words visited
     unsigned long long completions; // exact completions run
     unsigned long long tests;       // plane-window comparisons (stage x plane) executed

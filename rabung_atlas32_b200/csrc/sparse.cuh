@@ -34,16 +34,21 @@
 //
 // B200 design: one persistent kernel over all profiles of a call, handed out
 // longest first; a group of CTAs (2 for large calls, up to 64 when a call has
-// few profiles) shares one (p, r) profile, its warps pull rows d in increasing
-// order from the profile's counter in global memory and re-read the verified
-// maximum at every row, so the threshold rises while the profile runs; each
-// stored plane count has its own row loop (its own registers); lanes take
-// consecutive 64-anchor words of a row, a window is cut from three plane words
-// by funnel shifts, fetched through the load/store pipe for 1 and 2 planes and
-// through the texture pipe (linear textures over the plane pool) for 4 planes,
-// so the two L1 pipes share the load; words that survive are queued per warp
-// (across rows) and screened 32 at a time, one per lane, and the screened
-// candidates are completed 32 at a time, one per lane.
+// few profiles) shares one (p, r) profile.  A profile's rows d are cut into
+// epochs of consecutive d, each run with one threshold q -- the verified
+// maximum (or the speculative threshold) when the epoch's first work item is
+// claimed -- so the threshold rises between epochs and every row keeps one q.
+// A work item is (epoch, view, tile): the rows of the epoch whose parity reads
+// that view, restricted to the anchor bands that start in one tile of the
+// view's index range.  The tile's plane words, with the halo the t stages read
+// to its left and the band width to its right, are staged into shared memory
+// by one bulk asynchronous copy (cp.async.bulk, completed on an mbarrier), so
+// every anchor-stage window is a shared-memory load instead of an L1/L2 one.
+// Warps claim the item's rows from a shared counter; lanes take consecutive
+// 64-anchor words of a row; a window is cut from three plane words by funnel
+// shifts; words that survive are queued per warp (across rows and items of a
+// profile) and screened 32 at a time, one per lane, against the planes in
+// global memory, and the screened candidates are completed 32 at a time.
 #pragma once
 #include "labels.cuh"
 
@@ -62,16 +67,19 @@ namespace cz {
 #define CZ_SPARSE_MINB 2
 #endif
 
-#ifndef CZ_TEX_MASK                   // stored plane counts (bit NPP) whose windows go through textures
-#define CZ_TEX_MASK 4
+#ifndef CZ_TILE_WORDS                 // shared-memory tile of one work item, 32-bit words (all planes)
+#define CZ_TILE_WORDS 20480           // 80 KiB: two filter CTAs per SM
 #endif
-constexpr u32 TEX_CHUNK_WORDS_LOG2 = 27;   // texture chunks of the plane pool: 2^27 words (512 MiB)
+constexpr u32 TILE_WORDS = CZ_TILE_WORDS;
+constexpr u32 EPOCH_ROWS_DEFAULT = 256;     // rows d per threshold epoch
+constexpr u32 MBAR_SPIN_LIMIT = 1u << 22;   // bounded wait on a tile copy
 
 #ifndef CZ_SPARSE_WARPS               // warps per filter CTA
 #define CZ_SPARSE_WARPS 16
 #endif
 constexpr int SPARSE_WARPS = CZ_SPARSE_WARPS;
-constexpr int CAND_CAP = 64;          // per-warp buffers
+constexpr int CAND_CAP = 64;          // per-warp buffer of candidates awaiting completion
+constexpr int SCR_CAP = 96;           // per-warp buffer of words awaiting the screen (< 32 + two half-words of 32)
 constexpr u32 RUN_CAP = 4096;         // longest run a completion may walk
 
 struct Tuning {
@@ -88,8 +96,7 @@ struct SparseArgs {
     u32 *next;                // work counter: CTA slots handed out
     u32 group;                // CTAs that share one profile (its rows)
     Tuning tune;
-    const unsigned long long *texs;   // linear textures over the plane pool: [uint, uint2, uint4][chunk]
-    u32 tex_chunks;
+    u32 epoch_rows;           // rows d per threshold epoch
 };
 
 struct Cand { u32 b, d; };
@@ -104,19 +111,12 @@ CZ_HD u32 anchor_pref(u32 r, u32 bits) {
     return k + 1u;
 }
 
-// windows of all NPP interleaved planes at bit index u
+// 32-bit windows of all NPP interleaved planes at bit index u (global memory; the screen)
 template <int NPP> struct Planes;
 template <> struct Planes<1> {
     static __device__ __forceinline__ void win(const u32 *__restrict__ P, u32 u, u32 *o) {
         const u32 *q = P + (u >> 5);
         o[0] = __funnelshift_r(__ldg(q), __ldg(q + 1), u & 31u);
-    }
-    // 64-bit window: lo = bits [u, u+32), hi = bits [u+32, u+64)
-    static __device__ __forceinline__ void win64(const u32 *__restrict__ P, u32 u, u32 *lo, u32 *hi) {
-        const u32 *q = P + (u >> 5);
-        const u32 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), sh = u & 31u;
-        lo[0] = __funnelshift_r(a, b, sh);
-        hi[0] = __funnelshift_r(b, c, sh);
     }
 };
 template <> struct Planes<2> {
@@ -125,13 +125,6 @@ template <> struct Planes<2> {
         const uint2 a = __ldg(q), b = __ldg(q + 1);
         o[0] = __funnelshift_r(a.x, b.x, u & 31u);
         o[1] = __funnelshift_r(a.y, b.y, u & 31u);
-    }
-    static __device__ __forceinline__ void win64(const u32 *__restrict__ P, u32 u, u32 *lo, u32 *hi) {
-        const uint2 *q = reinterpret_cast<const uint2 *>(P) + (u >> 5);
-        const uint2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-        const u32 sh = u & 31u;
-        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
-        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
     }
 };
 template <> struct Planes<4> {
@@ -174,8 +167,11 @@ struct ProfCtx {
     u32 om[9];
     u32 seed, qspec;       // certified stretch from the table, speculative threshold
     u32 tpref;             // preferred anchor stages for this order
-    unsigned long long btex, otex;   // textures of the chunks holding the base / odd view
-    u32 btoff, otoff;                // uint4 element of each view's word 0 in its chunk
+    u32 NW2;               // odd view words per plane
+    u32 tmax;              // most anchor stages a row of this profile runs
+    u32 ts[2];             // tile span (anchor indices) of the base / odd view
+    u32 nt[2];             // tiles per epoch of each view
+    u32 nepoch, nitems;    // epochs, work items
 };
 
 // colour of numerator n (|n| <= B) as an integer, from the base view
@@ -329,7 +325,9 @@ __device__ __forceinline__ void screen_batch(const ProfCtx &c, uint4 *sb, Cand *
         if (screen && h > 0u) keep = screen_word<NPP>(v, i0, keep, d / v.G, t, h);
     }
     __syncwarp();
-    if (q.nscr > count && (u32)lane < q.nscr - count) sb[lane] = sb[count + lane];
+    // shift the rest down (up to SCR_CAP - 32 entries; each lane moves its own
+    // entries in order, so no lane overwrites one another lane still reads)
+    for (u32 i = (u32)lane; i + count < q.nscr; i += 32u) sb[i] = sb[count + i];
     __syncwarp();
     q.nscr -= count;
     while (__any_sync(0xFFFFFFFFu, keep != 0u)) {
@@ -347,11 +345,10 @@ __device__ __forceinline__ void screen_batch(const ProfCtx &c, uint4 *sb, Cand *
     }
 }
 
-// queue one 32-bit half-word per lane for the batched screen (the batch runs
-// as soon as 32 are waiting)
-template <int NPP>
-__device__ __forceinline__ void queue_words(const ProfCtx &c, uint4 *sb, Cand *cb, WarpQ &q, u32 i0, u32 alive,
-                                            u32 d, u32 t, bool screen, ProfState *st, int lane) {
+
+// queue one 32-bit half-word per lane for the batched screen; the caller runs
+// the screen once 32 are waiting (the buffer holds SCR_CAP)
+__device__ __forceinline__ void queue_append(uint4 *sb, WarpQ &q, u32 i0, u32 alive, u32 d, u32 t, int lane) {
     const bool has = alive != 0u;
     const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
     if (!bal) return;
@@ -359,96 +356,142 @@ __device__ __forceinline__ void queue_words(const ProfCtx &c, uint4 *sb, Cand *c
     if (has) sb[q.nscr + pos] = make_uint4(i0, alive, d, t);
     q.nscr += __popc(bal);
     __syncwarp();
-    if (q.nscr >= 32u) screen_batch<NPP>(c, sb, cb, q, 32u, screen, st, lane);
 }
 
-// the NPP words of texel e of a linear texture whose texels hold NPP words
-template <int NPP> struct Texel;
-template <> struct Texel<1> {
-    static __device__ __forceinline__ void get(unsigned long long t, int e, u32 *w) {
-        w[0] = tex1Dfetch<unsigned int>(t, e);
-    }
-};
-template <> struct Texel<2> {
-    static __device__ __forceinline__ void get(unsigned long long t, int e, u32 *w) {
-        const uint2 x = tex1Dfetch<uint2>(t, e);
-        w[0] = x.x; w[1] = x.y;
-    }
-};
-template <> struct Texel<4> {
-    static __device__ __forceinline__ void get(unsigned long long t, int e, u32 *w) {
-        const uint4 x = tex1Dfetch<uint4>(t, e);
-        w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
-    }
-};
+// ---- shared-memory tile: addresses, loads, bulk copy, mbarrier -------------
 
-// 64-bit window lo = bits [u, u+32), hi = bits [u+32, u+64) of a view.
-// Windows of the plane counts in CZ_TEX_MASK are fetched through the texture
-// pipe of the L1 unit (three texels from a linear texture over the plane
-// pool; u then counts from the texture chunk's element 0), the others through
-// the load/store pipe: the filter is bound by load/store wavefronts, and the
-// texture pipe next to it would otherwise stay idle, so profiles of different
-// plane counts stop competing for one pipe.
-template <int NPP>
-__device__ __forceinline__ void win64(const View &v, unsigned long long tex, u32 u, u32 *lo, u32 *hi) {
-    if constexpr ((CZ_TEX_MASK & NPP) != 0) {
-        const int e = (int)(u >> 5);
-        u32 a[NPP], b[NPP], c[NPP];
-        Texel<NPP>::get(tex, e, a);
-        Texel<NPP>::get(tex, e + 1, b);
-        Texel<NPP>::get(tex, e + 2, c);
-        const u32 sh = u & 31u;
-#pragma unroll
-        for (int k = 0; k < NPP; ++k) {
-            lo[k] = __funnelshift_r(a[k], b[k], sh);
-            hi[k] = __funnelshift_r(b[k], c[k], sh);
-        }
-    } else {
-        Planes<NPP>::win64(v.P, u, lo, hi);
-    }
+__device__ __forceinline__ u32 smem_addr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+
+// plain shared-memory loads at a shared-window byte address
+__device__ __forceinline__ u32 lds32(u32 a) {
+    u32 v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ uint2 lds64(u32 a) {
+    uint2 v;
+    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ uint4 lds128(u32 a) {
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+    return v;
 }
 
-// 64-bit mismatch mask (hi:lo) of a window against the base windows
+__device__ __forceinline__ void mbar_init(u32 mbar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(mbar), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// one arrival that also announces `bytes` of transaction to come
+__device__ __forceinline__ void mbar_expect_tx(u32 mbar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(u32 mbar, u32 parity) {
+    u32 ok;
+    asm volatile("{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\tselp.u32 %0, 1, 0, P;\n}"
+                 : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+    return ok != 0u;
+}
+// bounded wait for phase `parity` of the tile barrier; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait_bounded(u32 mbar, u32 parity) {
+    for (u32 i = 0; i < MBAR_SPIN_LIMIT; ++i)
+        if (mbar_try_wait(mbar, parity)) return true;
+    return false;
+}
+// bulk asynchronous copy global -> this CTA's shared memory (no multicast);
+// dst, src 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_load(u32 dst, const void *src, u32 bytes, u32 mbar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
+// 64-bit window lo = bits [u, u+32), hi = bits [u+32, u+64) of the NPP
+// interleaved planes of a tile at shared byte address S (word w of plane k at
+// S + 4 (w NPP + k))
+template <int NPP> struct Tile;
+template <> struct Tile<1> {
+    static __device__ __forceinline__ void win64(u32 S, u32 u, u32 *lo, u32 *hi) {
+        const u32 a0 = S + 4u * (u >> 5), sh = u & 31u;
+        const u32 a = lds32(a0), b = lds32(a0 + 4u), c = lds32(a0 + 8u);
+        lo[0] = __funnelshift_r(a, b, sh);
+        hi[0] = __funnelshift_r(b, c, sh);
+    }
+};
+template <> struct Tile<2> {
+    static __device__ __forceinline__ void win64(u32 S, u32 u, u32 *lo, u32 *hi) {
+        const u32 a0 = S + 8u * (u >> 5), sh = u & 31u;
+        const uint2 a = lds64(a0), b = lds64(a0 + 8u), c = lds64(a0 + 16u);
+        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
+        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
+    }
+};
+template <> struct Tile<4> {
+    static __device__ __forceinline__ void win64(u32 S, u32 u, u32 *lo, u32 *hi) {
+        const u32 a0 = S + 16u * (u >> 5), sh = u & 31u;
+        const uint4 a = lds128(a0), b = lds128(a0 + 16u), c = lds128(a0 + 32u);
+        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
+        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
+        lo[2] = __funnelshift_r(a.z, b.z, sh); hi[2] = __funnelshift_r(b.z, c.z, sh);
+        lo[3] = __funnelshift_r(a.w, b.w, sh); hi[3] = __funnelshift_r(b.w, c.w, sh);
+    }
+};
+
+// 64-bit mismatch mask (hi:lo) of a tile window against the base windows
 template <int NPP>
-__device__ __forceinline__ u64 mismatch64(const View &v, unsigned long long tex, u32 u, const u32 *blo,
-                                          const u32 *bhi) {
+__device__ __forceinline__ u64 mismatch64(u32 S, u32 u, const u32 *blo, const u32 *bhi) {
     u32 lo[NPP], hi[NPP];
-    win64<NPP>(v, tex, u, lo, hi);
+    Tile<NPP>::win64(S, u, lo, hi);
     u32 ml = 0, mh = 0;
 #pragma unroll
     for (int k = 0; k < NPP; ++k) { ml |= lo[k] ^ blo[k]; mh |= hi[k] ^ bhi[k]; }
     return ((u64)mh << 32) | ml;
 }
 
-// all selected words of row d on view v, 64 anchors per lane-word: per stage
-// three plane words, two funnel shifts and two logic ops per plane test 64
-// anchors, so ALU work and L1 requests per anchor-stage drop against 32-bit
-// words for a few more stages per word
+// one work item as staged in shared memory
+struct Item {
+    u32 S;             // shared byte address of the tile's first word
+    u32 ubase;         // view bit held by the tile's first word (32 x first view word)
+    u32 T0, T1;        // band starts in [T0, T1) (view indices) belong to this item
+    u32 view;          // 0 base (odd d), 1 odd view (even d)
+    u32 d0, nrows;     // rows d0, d0 + 2, ... (nrows of them)
+    u32 t, s;          // anchor stages, anchor spacing of the epoch
+};
+
+// the words of row d whose bands start in the item's tile: 64 anchors per
+// lane-word, every stage window read from shared memory.  Survivors are only
+// queued here; when 32 half-words wait for the screen the loop stops at rank
+// `base` and returns false, so the caller screens them with none of this
+// loop's state live and then resumes the row (true: the row is done)
 template <int NPP>
-__device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref, u32 d, u32 t, u32 s,
-                                             const Tuning &tune, uint4 *sb, Cand *cb, WarpQ &q, ProfState *st,
-                                             int lane, unsigned long long tex = 0ull, u32 tbits = 0u) {
-    const View v = vref;
-    const u32 G = v.G, dd = d / G;
+__device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u32 d, u32 &base, uint4 *sb,
+                                                WarpQ &q, int lane) {
+    const u32 G = v.G, dd = d / G, t = it.t;
     const u32 beta = ((t - 1u) * d + 1u) >> 1;
-    const i32 istart = (i32)((beta >= v.c ? beta - v.c + G - 1u : 0u) / G);
-    if (istart > v.ihi) return;
-    const u32 step = dd * s;
-    const u32 K = (u32)(v.ihi - istart) / step + 1u;
+    const u32 istart = (beta >= v.c ? beta - v.c + G - 1u : 0u) / G;
+    if ((i32)istart > v.ihi || istart >= it.T1) return true;
+    const u32 step = dd * it.s;
+    const u32 K = ((u32)v.ihi - istart) / step + 1u;
+    const u32 klo = it.T0 > istart ? (it.T0 - istart + step - 1u) / step : 0u;
+    const u32 khi = min(K, (it.T1 - istart + step - 1u) / step);
+    if (klo >= khi) return true;
     const u32 nw = (dd + 63u) >> 6;
-    const u32 W = K * nw;
-    const float rnw = 1.0f / (float)nw;
-    const bool screen = tune.screen != 0u;
-    for (u32 base = 0; base < W; base += 32u) {
+    const u32 W = (khi - klo) * nw;
+    const u32 mg = 0xFFFFFFFFu / nw + 1u;            // rank / nw by a multiply-high, fixed up below
+    const u32 ubias = v.OFF - it.ubase;
+    const u32 S = it.S;
+    while (base < W) {
         const u32 rank = base + (u32)lane;
+        base += 32u;
         u64 alive = 0;
         u32 i0 = 0;
         if (rank < W) {
-            u32 k = (u32)((float)rank * rnw);
+            u32 k = nw == 1u ? rank : umulhi(rank, mg);
             if (k * nw > rank) --k;
             else if ((k + 1u) * nw <= rank) ++k;
             const u32 w = rank - k * nw;
-            i0 = (u32)istart + k * step + 64u * w;
+            i0 = istart + (klo + k) * step + 64u * w;
             u32 len = dd - 64u * w;
             if (len > 64u) len = 64u;
             if ((i32)i0 > v.ihi) len = 0;
@@ -457,109 +500,217 @@ __device__ __forceinline__ void filter_row64(const ProfCtx &c, const View &vref,
         }
         if (alive) {
             ++q.words;
-            const u32 u = i0 + v.OFF + tbits;        // tbits: texture chunk offset (4 planes), else 0
+            const u32 u = i0 + ubias;                // tile bit of the anchor word
             u32 blo[NPP], bhi[NPP];
-            win64<NPP>(v, tex, u, blo, bhi);
+            Tile<NPP>::win64(S, u, blo, bhi);
             constexpr int SB = NPP == 4 ? CZ_SB4 : (NPP == 2 ? CZ_SB2 : CZ_SB1);
             u32 j = 1;
             while (j < t && alive) {
                 u64 m[SB];
 #pragma unroll
                 for (int k = 0; k < SB; ++k)
-                    m[k] = (j + (u32)k < t) ? mismatch64<NPP>(v, tex, u - (j + (u32)k) * dd, blo, bhi) : 0ull;
+                    m[k] = (j + (u32)k < t) ? mismatch64<NPP>(S, u - (j + (u32)k) * dd, blo, bhi) : 0ull;
 #pragma unroll
                 for (int k = 0; k < SB; ++k) alive &= ~m[k];
                 j += SB;
             }
             q.tests += 2u * min(j, t) * (u32)NPP;
         }
-        queue_words<NPP>(c, sb, cb, q, i0, (u32)alive, d, t, screen, st, lane);
-        queue_words<NPP>(c, sb, cb, q, i0 + 32u, (u32)(alive >> 32), d, t, screen, st, lane);
+        queue_append(sb, q, i0, (u32)alive, d, t, lane);
+        queue_append(sb, q, i0 + 32u, (u32)(alive >> 32), d, t, lane);
+        if (q.nscr >= 32u) return base >= W;
+    }
+    return true;
+}
+
+// the rows of the staged item, claimed one per warp from a shared counter
+template <int NPP>
+__device__ __forceinline__ void filter_item(const ProfCtx &c, const Item &it, const SparseArgs &a, u32 *row_ctr,
+                                            uint4 *sb, Cand *cb, WarpQ &q, ProfState *st, int lane) {
+    const bool screen = a.tune.screen != 0u;
+    for (;;) {
+        u32 r = 0;
+        if (lane == 0) r = atomicAdd(row_ctr, 1u);
+        r = __shfl_sync(0xFFFFFFFFu, r, 0);
+        if (r >= it.nrows) break;
+        const u32 d = it.d0 + 2u * r;
+        u32 base = 0;
+        for (;;) {
+            const bool done = filter_row_tile<NPP>(it.view ? c.odd : c.base, it, d, base, sb, q, lane);
+            while (q.nscr >= 32u) screen_batch<NPP>(c, sb, cb, q, 32u, screen, st, lane);
+            if (done) break;
+            asm volatile("" ::: "memory");            // row state is recomputed, not kept across the screen
+        }
     }
 }
 
-// the rows of one profile, handed out one per warp in increasing d
-template <int NPP>
-__device__ __forceinline__ void filter_rows(const ProfCtx &c, const SparseArgs &a, u32 tpref, uint4 *sb, Cand *cb,
-                                            WarpQ &q, ProfState *st, int lane) {
-    for (;;) {
-        u32 d = 0;
-        if (lane == 0) d = atomicAdd(&st->rows_next, 1u) + 1u;     // rows in increasing d
-        d = __shfl_sync(0xFFFFFFFFu, d, 0);
-        if (d > c.D) break;
-        // row parameters from the verified maximum so far (<= M); with a
-        // speculative threshold every run >= it is still completed, and a
-        // profile whose best stays below it is re-run without it
-        const u32 blen = threshold(c, st);
-        const u32 q_ = blen < c.Q ? blen : c.Q;
-        if (q_ < 3u) { q.err |= 2u; break; }
-        const u32 t = tpref < q_ ? (tpref < 2u ? 2u : tpref) : q_;
-        const u32 s = q_ - t + 1u;
-        const View &v = (d & 1u) ? c.base : c.odd;
-        if constexpr ((CZ_TEX_MASK & NPP) != 0)
-            filter_row64<NPP>(c, v, d, t, s, a.tune, sb, cb, q, st, lane, (d & 1u) ? c.btex : c.otex,
-                              32u * ((d & 1u) ? c.btoff : c.otoff));
-        else
-            filter_row64<NPP>(c, v, d, t, s, a.tune, sb, cb, q, st, lane);
+// tiling of a profile: per view, the span of anchor indices one tile holds
+// (its words plus the left halo of tmax - 1 row steps, the right halo of one
+// band and the window's two extra words fit TILE_WORDS / NPP words), tiles per
+// epoch, epochs and items; false if a view cannot be tiled
+__device__ inline bool plan_tiles(ProfCtx &c, u32 epoch_rows) {
+    const u32 cap_bits = 32u * (TILE_WORDS / c.npp - 16u);
+    for (u32 v = 0; v < 2; ++v) {
+        const u32 G = v ? 2u : 1u;
+        const u32 ddmax = (c.D + G - 1u) / G;
+        const u64 halo = (u64)c.tmax * ddmax + 320u;
+        if (halo + 1024u > cap_bits) return false;
+        const u32 span = ((cap_bits - (u32)halo) / 64u) * 64u;
+        const i32 ihi = v ? c.odd.ihi : c.base.ihi;
+        const u32 extent = ihi >= 0 ? (u32)ihi + 1u : 0u;       // anchor band starts lie in [0, ihi]
+        c.nt[v] = (extent + span - 1u) / span;
+        c.ts[v] = c.nt[v] ? ((extent + c.nt[v] - 1u) / c.nt[v] + 63u) / 64u * 64u : span;
     }
+    c.nepoch = (c.D + epoch_rows - 1u) / epoch_rows;
+    c.nitems = c.nepoch * (c.nt[0] + c.nt[1]);
+    return true;
+}
+
+// claim the next work item of profile st (thread 0): a 64-bit state holds the
+// next item (low 32 bits), and the epoch (bits 32..47, + 1) and threshold
+// (bits 48..55) fixed by the first claim of the current epoch
+__device__ inline bool claim_item(const ProfCtx &c, ProfState *st, u32 &item, u32 &qe) {
+    unsigned long long old = *(volatile unsigned long long *)&st->claim;
+    const u32 ipe = c.nt[0] + c.nt[1];
+    for (int guard = 0; guard < 1 << 20; ++guard) {
+        item = (u32)old;
+        if (item >= c.nitems) return false;
+        const u32 e = item / ipe;
+        unsigned long long nw;
+        if ((u32)((old >> 32) & 0xFFFFu) == e + 1u) {
+            qe = (u32)((old >> 48) & 0xFFu);
+            nw = old + 1ull;
+        } else {
+            const u32 thr = threshold(c, st);
+            qe = thr < c.Q ? thr : c.Q;
+            nw = ((unsigned long long)qe << 48) | ((unsigned long long)(e + 1u) << 32) | (item + 1u);
+        }
+        const unsigned long long prev = atomicCAS(&st->claim, old, nw);
+        if (prev == old) return true;
+        old = prev;
+    }
+    return false;
+}
+
+// thread 0: claim the profile's next work item, describe it in *out and start
+// the bulk copy of its tile into shared memory; false when the profile has no
+// item left (or on an error, reported in *err: 2 threshold below 3, 4 tile)
+__device__ __noinline__ bool next_item(const ProfCtx &c, ProfState *st, u32 erows, u32 tile, u32 mbar, Item *out,
+                                       u32 *err) {
+    u32 item = 0, qe = 0;
+    if (!claim_item(c, st, item, qe)) return false;
+    if (qe < 3u) { *err |= 2u; return false; }
+    Item it;
+    const u32 ipe = c.nt[0] + c.nt[1], e = item / ipe, j = item - e * ipe;
+    it.view = j < c.nt[0] ? 0u : 1u;
+    const u32 k = it.view ? j - c.nt[0] : j;
+    const View &v = it.view ? c.odd : c.base;
+    const u32 G = v.G;
+    it.T0 = k * c.ts[it.view];
+    it.T1 = min(it.T0 + c.ts[it.view], (u32)v.ihi + 1u);
+    it.t = c.tpref < qe ? c.tmax : qe;
+    it.s = qe - it.t + 1u;
+    // rows of the epoch with the view's parity: d odd (base), d even (odd view)
+    const u32 dlo = e * erows + 1u, dhi = min(c.D, (e + 1u) * erows);
+    it.d0 = (dlo & 1u) == (it.view ? 0u : 1u) ? dlo : dlo + 1u;
+    it.nrows = it.d0 <= dhi ? (dhi - it.d0) / 2u + 1u : 0u;
+    const u32 ddmax = dhi / G;
+    // view words the item reads: left halo (t - 1) row steps, right halo one band + window
+    const i64 lob = (i64)it.T0 + v.OFF - (i64)(it.t - 1u) * ddmax - 32;
+    const u64 hib = (u64)it.T1 + v.OFF + ddmax + 128u;
+    const u32 nwv = it.view ? c.NW2 : c.NW;
+    const u32 w0 = lob > 0 ? (u32)(lob >> 5) & ~3u : 0u;
+    const u64 w1r = ((hib >> 5) + 4u) & ~3ull;
+    u32 w1 = w1r < (u64)nwv ? (u32)w1r : nwv;
+    if (w1 < w0 + 4u) w1 = min(nwv, w0 + 4u);
+    const u32 bytes = (w1 - w0) * c.npp * 4u;
+    if (bytes > TILE_WORDS * 4u || w1 <= w0) { *err |= 4u; return false; }
+    it.S = tile;
+    it.ubase = 32u * w0;
+    *out = it;
+    mbar_expect_tx(mbar, bytes);
+    bulk_load(tile, v.P + (size_t)w0 * c.npp, bytes, mbar);
+    return true;
+}
+
+// thread 0: the per-profile constants of global profile gprof, and its tiling
+__device__ __noinline__ void load_profile(const SparseArgs &a, u32 gprof, ProfCtx *out, u32 *err) {
+    const ProfDesc PD = a.profs[gprof];
+    const PrimeDesc PR = a.primes[PD.prime];
+    ProfCtx c;
+    c.p = PR.p; c.r = PD.r; c.np = PD.np; c.npp = PD.npp; c.Q = PD.Q; c.D = PD.D; c.B = PR.B;
+    c.NW = PR.nwords; c.NW2 = PR.nwords2; c.OFF = 32u * PR.K0 + 31u; c.ex = (PR.p - 1u) / PD.r;
+    c.M = Mont{PR.p, PR.ninv, PR.one, PR.r2};
+    c.P = a.planes + PD.plane_off;
+    c.base = View{c.P, c.OFF, -(i32)PR.B, (i32)PR.B, 1u, 0u};
+    // odd view: n = 2i + 1 in [-B, B]  <=>  i in [ceil((-B-1)/2), floor((B-1)/2)]
+    c.odd = View{c.P + (size_t)PR.nwords * PD.npp, 32u * PR.K2, -(i32)((PR.B + 1u) / 2u), (i32)((PR.B - 1u) / 2u),
+                 2u, 1u};
+    for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
+    c.seed = *(volatile u32 *)&a.state[gprof].seed;
+    c.qspec = PD.qspec;
+    c.tpref = PD.tpref;
+    c.tmax = c.tpref < 2u ? 2u : c.tpref;
+    if (!plan_tiles(c, a.epoch_rows ? a.epoch_rows : EPOCH_ROWS_DEFAULT)) { c.nitems = 0; *err |= 4u; }
+    *out = c;
 }
 
 __global__ void __launch_bounds__(SPARSE_WARPS * 32, CZ_SPARSE_MINB)
 sparse_kernel(SparseArgs a) {
-    __shared__ u32 s_item, s_err;
+    extern __shared__ __align__(128) uint4 s_tile[];   // TILE_WORDS words
+    __shared__ unsigned long long s_mbar;
+    __shared__ u32 s_item, s_err, s_row, s_has, s_phase;
     __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];      // candidates awaiting completion
-    __shared__ uint4 sbuf[SPARSE_WARPS][CAND_CAP];     // (index, alive, d, t) words awaiting the screen
+    __shared__ uint4 sbuf[SPARSE_WARPS][SCR_CAP];      // (index, alive, d, t) words awaiting the screen
     __shared__ ProfCtx s_ctx;
+    __shared__ Item s_it;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_addr(&s_mbar), 1u);
+        s_phase = 0u;                                  // tile copies completed so far
+    }
+    __syncthreads();
     for (;;) {
         if (threadIdx.x == 0) {
             // a.group consecutive CTA slots share one profile
             s_item = atomicAdd(a.next, 1u) / a.group;
             s_err = 0u;
-            if (s_item < a.nlist) {
-                const u32 gprof = a.prof_list[s_item];
-                const ProfDesc PD = a.profs[gprof];
-                const PrimeDesc PR = a.primes[PD.prime];
-                ProfCtx c;
-                c.p = PR.p; c.r = PD.r; c.np = PD.np; c.npp = PD.npp; c.Q = PD.Q; c.D = PD.D; c.B = PR.B;
-                c.NW = PR.nwords; c.OFF = 32u * PR.K0 + 31u; c.ex = (PR.p - 1u) / PD.r;
-                c.M = Mont{PR.p, PR.ninv, PR.one, PR.r2};
-                c.P = a.planes + PD.plane_off;
-                c.base = View{c.P, c.OFF, -(i32)PR.B, (i32)PR.B, 1u, 0u};
-                // odd view: n = 2i + 1 in [-B, B]  <=>  i in [ceil((-B-1)/2), floor((B-1)/2)]
-                c.odd = View{c.P + (size_t)PR.nwords * PD.npp, 32u * PR.K2, -(i32)((PR.B + 1u) / 2u),
-                             (i32)((PR.B - 1u) / 2u), 2u, 1u};
-                {
-                    const u64 bb = (u64)PD.plane_off * 4ull;
-                    const u64 ob = bb + (u64)PR.nwords * PD.npp * 4ull;
-                    const u32 f = PD.npp == 1u ? 0u : (PD.npp == 2u ? 1u : 2u), sh = TEX_CHUNK_WORDS_LOG2 + 2u;
-                    const u64 msk = (1ull << sh) - 1ull, tb = 4ull * PD.npp;   // bytes per texel
-                    c.btex = __ldg(a.texs + f * a.tex_chunks + (bb >> sh));
-                    c.btoff = (u32)((bb & msk) / tb);
-                    c.otex = __ldg(a.texs + f * a.tex_chunks + (ob >> sh));
-                    c.otoff = (u32)((ob & msk) / tb);
-                }
-                for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
-                c.seed = *(volatile u32 *)&a.state[gprof].seed;
-                c.qspec = PD.qspec;
-                c.tpref = PD.tpref;
-                s_ctx = c;
-            }
+            if (s_item < a.nlist) load_profile(a, a.prof_list[s_item], &s_ctx, &s_err);
         }
         __syncthreads();
-        const u32 item = s_item;
-        if (item >= a.nlist) return;
+        const u32 pitem = s_item;
+        if (pitem >= a.nlist) return;
         const ProfCtx &c = s_ctx;
-        ProfState *st = a.state + a.prof_list[item];
-        const u32 tpref = c.tpref;
+        ProfState *st = a.state + a.prof_list[pitem];
         WarpQ q{0, 0, 0, 0, 0, 0, 0};
         uint4 *sb = sbuf[warp];
         Cand *cb = cbuf[warp];
-        // one row loop per stored plane count, so each keeps its own registers
-        if (c.npp == 1u) filter_rows<1>(c, a, tpref, sb, cb, q, st, lane);
-        else if (c.npp == 2u) filter_rows<2>(c, a, tpref, sb, cb, q, st, lane);
-        else filter_rows<4>(c, a, tpref, sb, cb, q, st, lane);
-        // the screen queue carries across rows: drain it, then the candidates
+        for (;;) {
+            if (threadIdx.x == 0) {
+                u32 err = 0;
+                s_has = next_item(c, st, a.epoch_rows ? a.epoch_rows : EPOCH_ROWS_DEFAULT, smem_addr(s_tile),
+                                  smem_addr(&s_mbar), &s_it, &err) ? 1u : 0u;
+                s_err |= err;
+                s_row = 0u;
+            }
+            __syncthreads();
+            if (!s_has) break;
+            // wait for the tile copy (bounded); the verdict is made CTA-uniform
+            const u32 par = s_phase & 1u;
+            const bool ok = __syncthreads_and(mbar_wait_bounded(smem_addr(&s_mbar), par) ? 1 : 0) != 0;
+            if (!ok) {
+                if (threadIdx.x == 0) atomicOr(&st->status, ST_QUEUE);
+                mbar_wait_bounded(smem_addr(&s_mbar), par);    // let the copy land before leaving
+                return;
+            }
+            const Item &it = s_it;
+            if (c.npp == 1u) filter_item<1>(c, it, a, &s_row, sb, cb, q, st, lane);
+            else if (c.npp == 2u) filter_item<2>(c, it, a, &s_row, sb, cb, q, st, lane);
+            else filter_item<4>(c, it, a, &s_row, sb, cb, q, st, lane);
+            if (threadIdx.x == 0) s_phase += 1u;
+            __syncthreads();                               // the tile is free for the next copy
+        }
+        // the screen queue carries across rows and items: drain it, then the candidates
         if (q.nscr) {
             if (c.npp == 1u) screen_batch<1>(c, sb, cb, q, q.nscr, a.tune.screen != 0u, st, lane);
             else if (c.npp == 2u) screen_batch<2>(c, sb, cb, q, q.nscr, a.tune.screen != 0u, st, lane);
@@ -575,7 +726,8 @@ sparse_kernel(SparseArgs a) {
             atomicAdd(&st->tests, (unsigned long long)tests);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && s_err) atomicOr(&st->status, (s_err & 2u) ? ST_SEED : ST_QUEUE);
+        if (threadIdx.x == 0 && s_err)
+            atomicOr(&st->status, (s_err & 2u) ? ST_SEED : ((s_err & 4u) ? ST_COVER : ST_QUEUE));
     }
 }
 

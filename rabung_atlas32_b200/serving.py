@@ -78,7 +78,7 @@ class Server:
             cfg.device = device
             cfg.sparse_min_p, cfg.cover_n, cfg.anchor_bits, cfg.screen = t.sparse_min_p, t.cover_n, t.anchor_bits, t.screen
             cfg.sparse_blocks, cfg.use_graph, cfg.cta_per_profile = t.sparse_blocks, t.use_graph, t.cta_per_profile
-            cfg.l1_carveout, cfg.speculate, cfg.plane_budget_mb = t.l1_carveout, t.speculate, t.plane_budget_mb
+            cfg.epoch_rows, cfg.speculate, cfg.plane_budget_mb = t.epoch_rows, t.speculate, t.plane_budget_mb
             cfg.dense_steps = t.dense_steps
             for r in range(10):
                 cfg.q_cap[r], cfg.spec_margin10[r], cfg.anchor_t[r] = t.q_cap[r], t.spec_margin10[r], t.anchor_t[r]

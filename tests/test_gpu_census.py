@@ -245,3 +245,44 @@ def test_reference_c_abi_baseline_profile(golden):
             assert lib.baseline_profile(rec.p, 0b11, out, pre, 0) == 2
             assert lib.baseline_profile(rec.p, 0b11, out, pre, 1) == 0
     assert checked > 100
+
+
+def test_epoch_rows_do_not_change_records():
+    """Rows per threshold epoch (one row per epoch up to one epoch per profile)
+    only change when the filter's threshold rises; the records are certified
+    either way and must not move."""
+    import dataclasses
+    from rabung_atlas32_b200.census import Census, Tuning
+    ps = sieve.primes_ending(4294967291, 48) + sieve.primes_from(1 << 24, 48)
+    with Census(tuning=Tuning()) as c0:
+        want = tup(c0.profiles(ps, mode="sparse", a4=False))
+    for er in (1, 7, 64, 1 << 20):
+        with Census(tuning=dataclasses.replace(Tuning(), epoch_rows=er)) as c1:
+            assert tup(c1.profiles(ps, mode="sparse", a4=False)) == want, er
+
+
+def test_small_tiles_do_not_change_records(tmp_path):
+    """A library built with 16 KiB shared-memory tiles (instead of 80 KiB) cuts
+    every view into many tiles (up to ~20 per view here), so bands, halos and
+    tile edges are crossed everywhere; its records must equal the default
+    build's, with no prime sent back to the dense path."""
+    import subprocess
+    from rabung_atlas32_b200 import _lib, build
+    from rabung_atlas32_b200.census import Census, Tuning
+    ps = sieve.primes_from(1 << 26, 40) + sieve.primes_from(1 << 28, 40) + sieve.primes_ending(1 << 30, 24)
+    with Census(tuning=Tuning()) as c0:
+        want = tup(c0.profiles(ps, mode="sparse", a4=False))
+    so = tmp_path / "librabung_census_tile4k.so"
+    cmd = [build.NVCC, *build.FLAGS, "-DCZ_TILE_WORDS=4096", "-I", str(build.ROOT / "include"), "-o", str(so),
+           str(build.CSRC / "census.cu")]
+    subprocess.run(cmd, check=True, capture_output=True)
+    lib = _lib.load(so)
+    saved = _lib._lib
+    try:
+        _lib._lib = lib
+        with Census(tuning=Tuning()) as c1:
+            got = c1.profiles(ps, mode="sparse", a4=False)
+            assert c1.last_stats["n_fallback"] == 0
+            assert tup(got) == want
+    finally:
+        _lib._lib = saved

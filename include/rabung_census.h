@@ -207,6 +207,27 @@ int cz_poll(cz_server *s, uint64_t request_id, int32_t timeout_ms, uint32_t *pri
 int cz_server_info(cz_server *s, uint64_t *batches, uint64_t *completed, uint64_t *waiting);
 const char *cz_server_last_error(cz_server *s);
 
+/* ---- the 33-bit domain -------------------------------------------------------
+ * The same census for primes below 2^33 (the reference's 33-bit engine,
+ * src/census/math33.hpp:13-37 and reproducibility/gpu_method/source/engine33):
+ * identical kernels and planning compiled for 64-bit prime words.  A record
+ * carries p in 64 bits; the canonical witness is at most (p-1)/2 < 2^32.
+ * Flags, refusal rules and statistics as for cz_census. */
+typedef struct cz_profile64 {
+    uint64_t p;
+    uint32_t r, M, L, witness, status, reserved;
+    uint64_t K;
+} cz_profile64;
+
+typedef struct cz_handle64 cz_handle64;
+int cz_open64(const cz_config *cfg, cz_handle64 **out);
+void cz_close64(cz_handle64 *h);
+const char *cz_last_error64(const cz_handle64 *h);
+/* profiles of n primes (0 when a prime is at or above 2^33) */
+uint32_t cz_count_profiles64(const uint64_t *primes, uint32_t n);
+int cz_census64(cz_handle64 *h, const uint64_t *primes, uint32_t n, uint32_t flags, cz_profile64 *out,
+                uint32_t out_cap, uint32_t *a4_out, cz_stats *stats);
+
 /* Reference-compatible adapter (src/census/engine32/src/baseline_bridge.cu:7,21-27):
  * profile of one prime for the orders in `mask` (bit r-2), M into out[r] and
  * L into prefix[r] (arrays of >= 10).  With full = 0 only the masks the

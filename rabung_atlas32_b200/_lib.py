@@ -23,6 +23,11 @@ class cz_profile(ctypes.Structure):
                 ("status", u32), ("K", u64)]
 
 
+class cz_profile64(ctypes.Structure):
+    _fields_ = [("p", u64), ("r", u32), ("M", u32), ("L", u32), ("witness", u32),
+                ("status", u32), ("reserved", u32), ("K", u64)]
+
+
 class cz_config(ctypes.Structure):
     _fields_ = [("device", i32), ("sparse_min_p", u32), ("cover_n", u32), ("q_cap", u32 * 10),
                 ("anchor_bits", u32), ("screen", u32), ("sparse_blocks", u32), ("use_graph", u32),
@@ -48,7 +53,8 @@ EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_coun
            "cz_census", "cz_replay", "cz_a4", "cz_sieve", "cz_plane_bytes", "cz_mem_info", "cz_device_info",
            "cz_microbench", "cz_census_dense_noalloc", "cz_census_interval", "cz_server_open",
            "cz_server_close", "cz_submit", "cz_next_done", "cz_poll", "cz_server_info", "cz_server_last_error",
-           "cz_prime_count", "baseline_init", "baseline_profile"]
+           "cz_prime_count", "cz_open64", "cz_close64", "cz_last_error64", "cz_count_profiles64", "cz_census64",
+           "baseline_init", "baseline_profile"]
 
 _lib = None
 
@@ -112,6 +118,17 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.cz_server_info.restype = ctypes.c_int
     L.cz_server_last_error.argtypes = [H]
     L.cz_server_last_error.restype = ctypes.c_char_p
+    L.cz_open64.argtypes = [ctypes.POINTER(cz_config), ctypes.POINTER(H)]
+    L.cz_open64.restype = ctypes.c_int
+    L.cz_close64.argtypes = [H]
+    L.cz_close64.restype = None
+    L.cz_last_error64.argtypes = [H]
+    L.cz_last_error64.restype = ctypes.c_char_p
+    L.cz_count_profiles64.argtypes = [ctypes.POINTER(u64), u32]
+    L.cz_count_profiles64.restype = u32
+    L.cz_census64.argtypes = [H, ctypes.POINTER(u64), u32, u32, ctypes.POINTER(cz_profile64), u32,
+                              ctypes.POINTER(u32), ctypes.POINTER(cz_stats)]
+    L.cz_census64.restype = ctypes.c_int
     L.cz_prime_count.argtypes = [u64, u64]
     L.cz_prime_count.restype = u64
     L.baseline_init.argtypes = [ctypes.c_uint]

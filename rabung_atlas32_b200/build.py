@@ -44,7 +44,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if LIB.exists() and not force and KEY.exists() and KEY.read_text().strip() == key:
         return LIB
     tmp = LIB.with_suffix(f".{os.getpid()}.tmp.so")
-    cmd = [NVCC, *FLAGS, "-I", str(ROOT / "include"), "-o", str(tmp), str(CSRC / "census.cu")]
+    cmd = [NVCC, *FLAGS, "-I", str(ROOT / "include"), "-o", str(tmp), str(CSRC / "census.cu"),
+           str(CSRC / "census_wide.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -67,6 +67,29 @@ def to_records(primes, out, a4v) -> list:
     return recs
 
 
+def config(lib, device: int, t: Tuning) -> "_lib.cz_config":
+    """The library configuration of a Tuning on `device`."""
+    cfg = _lib.cz_config()
+    lib.cz_default_config(ctypes.byref(cfg))
+    cfg.device = device
+    cfg.sparse_min_p = t.sparse_min_p
+    cfg.cover_n = t.cover_n
+    cfg.anchor_bits = t.anchor_bits
+    cfg.screen = t.screen
+    cfg.sparse_blocks = t.sparse_blocks
+    cfg.use_graph = t.use_graph
+    cfg.cta_per_profile = t.cta_per_profile
+    cfg.epoch_rows = t.epoch_rows
+    cfg.speculate = t.speculate
+    cfg.plane_budget_mb = t.plane_budget_mb
+    cfg.dense_steps = t.dense_steps
+    for r in range(10):
+        cfg.q_cap[r] = t.q_cap[r]
+        cfg.spec_margin10[r] = t.spec_margin10[r]
+        cfg.anchor_t[r] = t.anchor_t[r]
+    return cfg
+
+
 class Census:
     def __init__(self, device: int = 0, tuning: Tuning | None = None, autoload: bool = True):
         """Open a handle on `device`.  Without an explicit tuning, the
@@ -88,28 +111,8 @@ class Census:
         self._open(device, tuning or Tuning())
 
     def _open(self, device: int, t: Tuning):
-        cfg = _lib.cz_config()
-        self.lib.cz_default_config(ctypes.byref(cfg))
-        cfg.device = device
-        cfg.sparse_min_p = t.sparse_min_p
-        cfg.cover_n = t.cover_n
-        for r in range(10):
-            cfg.q_cap[r] = t.q_cap[r]
-        cfg.anchor_bits = t.anchor_bits
-        cfg.screen = t.screen
-        cfg.sparse_blocks = t.sparse_blocks
-        cfg.use_graph = t.use_graph
-        cfg.cta_per_profile = t.cta_per_profile
-        cfg.epoch_rows = t.epoch_rows
-        cfg.speculate = t.speculate
-        for r in range(10):
-            cfg.spec_margin10[r] = t.spec_margin10[r]
-        cfg.plane_budget_mb = t.plane_budget_mb
-        cfg.dense_steps = t.dense_steps
-        for r in range(10):
-            cfg.anchor_t[r] = t.anchor_t[r]
         h = ctypes.c_void_p()
-        rc = self.lib.cz_open(ctypes.byref(cfg), ctypes.byref(h))
+        rc = self.lib.cz_open(ctypes.byref(config(self.lib, device, t)), ctypes.byref(h))
         if rc != 0:
             raise CensusError(f"cz_open failed (rc={rc}): no usable CUDA device or bad tuning")
         self.h = h
@@ -252,6 +255,77 @@ class Census:
             primes = primes_in(lo, hi)
         recs = self.profiles(primes, mode=mode, a4=True, verify=verify)
         return codec.encode_scan_frame(lo, hi, recs), codec.encode_a4_frame(lo, hi, recs), recs
+
+
+class Census64:
+    """The census for primes below 2^33 (the reference's 33-bit domain):
+    cz_open64 / cz_census64, the same kernels compiled for 64-bit prime
+    words.  Same tuning, modes, A4, certification and refusal rules as
+    Census; records carry p as a Python int."""
+
+    def __init__(self, device: int = 0, tuning: Tuning | None = None):
+        self.lib = _lib.load()
+        self.h = None
+        if tuning is None:
+            with Census(device=device, autoload=True) as probe:
+                tuning = probe.tuning
+        h = ctypes.c_void_p()
+        rc = self.lib.cz_open64(ctypes.byref(config(self.lib, device, tuning)), ctypes.byref(h))
+        if rc != 0:
+            raise CensusError(f"cz_open64 failed (rc={rc}): no usable CUDA device or bad tuning")
+        self.h = h
+        self.tuning = tuning
+        self.last_stats: dict = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cz_close64(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _arr(primes):
+        arr = (ctypes.c_uint64 * max(1, len(primes)))()
+        for i, v in enumerate(primes):
+            if not 0 <= int(v) < 2 ** 33:
+                raise ValueError(f"prime out of the 33-bit domain: {v}")
+            arr[i] = int(v)
+        return arr
+
+    def count_profiles(self, primes) -> int:
+        return int(self.lib.cz_count_profiles64(self._arr(primes), len(primes)))
+
+    def raw(self, primes, mode: str = "auto", a4: bool = True, verify: bool = True):
+        """(ctypes cz_profile64 array, A4 list or None, stats dict)."""
+        n = len(primes)
+        arr = self._arr(primes)
+        nprof = int(self.lib.cz_count_profiles64(arr, n))
+        out = (_lib.cz_profile64 * max(1, nprof))()
+        a4buf = (ctypes.c_uint32 * max(1, n))() if a4 else None
+        flags = MODES[mode] | (_lib.CZ_A4 if a4 else 0) | (_lib.CZ_VERIFY if verify else 0)
+        st = _lib.cz_stats()
+        rc = self.lib.cz_census64(self.h, arr, n, flags, out, nprof, a4buf, ctypes.byref(st))
+        if rc != 0:
+            err = self.lib.cz_last_error64(self.h).decode(errors="replace")
+            raise CensusError(f"census refused (rc={rc}): {err}")
+        self.last_stats = st.as_dict()
+        return out, (list(a4buf[:n]) if a4 else None), self.last_stats
+
+    def profiles(self, primes, mode: str = "auto", a4: bool = True, verify: bool = True):
+        """List of codec.Record (profiles ascending r, A4 when requested)."""
+        out, a4v, _ = self.raw(primes, mode, a4, verify)
+        return to_records(primes, out, a4v)
 
 
 def main(argv=None):

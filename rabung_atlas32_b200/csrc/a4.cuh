@@ -16,47 +16,49 @@
 // the 32 lanes and hashed by x-coordinate in shared memory; giant steps
 // (L + i m) P are taken 32 at a time, one per lane; the point order is
 // found lane-parallel per prime factor of the matched multiple; all curve
-// arithmetic is affine in 32-bit Montgomery form with Fermat inverses.
+// arithmetic is affine in Montgomery form (the prime's word width) with
+// Fermat inverses.
 #pragma once
 #include "labels.cuh"
 
-namespace cz {
+namespace CZ_NS {
 
-constexpr int A4_WARPS = 4;
-constexpr u32 A4_SLOTS = 1024;      // hash slots per warp (m <= 513)
+constexpr int A4_WARPS = CZ_WIDE ? 2 : 4;   // primes per CTA (shared hash tables: 18 / 10 KB per warp)
+constexpr u32 A4_SLOTS = 1024;      // hash slots per warp (m <= 513 below 2^32, <= 610 below 2^33)
+constexpr pw_t NO_ROOT = ~(pw_t)0;
 constexpr u32 A4_MAX_ATTEMPTS = 64;
 
-struct ECPt { u32 x, y; bool inf; };
+struct ECPt { pw_t x, y; bool inf; };
 
 struct Curve {
     Mont M;
-    u32 s10, s9sq, s20, three;   // Montgomery 10s, 9s^2, 20s, 3
+    pw_t s10, s9sq, s20, three;  // Montgomery 10s, 9s^2, 20s, 3
 };
 
-__device__ __forceinline__ u32 addm(u32 a, u32 b, u32 p) { u64 c = (u64)a + b; return c >= p ? (u32)(c - p) : (u32)c; }
-__device__ __forceinline__ u32 subm(u32 a, u32 b, u32 p) { return a >= b ? a - b : (u32)((u64)a + p - b); }
-__device__ __forceinline__ u32 invm(u32 a, const Mont &M) { return mpow(a, M.p - 2u, M); }
+__device__ __forceinline__ pw_t addm(pw_t a, pw_t b, pw_t p) { u64 c = (u64)a + b; return c >= p ? (pw_t)(c - p) : (pw_t)c; }
+__device__ __forceinline__ pw_t subm(pw_t a, pw_t b, pw_t p) { return a >= b ? a - b : (pw_t)((u64)a + p - b); }
+__device__ __forceinline__ pw_t invm(pw_t a, const Mont &M) { return mpow(a, M.p - 2u, M); }
 
 __device__ ECPt ec_add(const ECPt &A, const ECPt &B, const Curve &E) {
     if (A.inf) return B;
     if (B.inf) return A;
     const Mont &M = E.M;
-    const u32 p = M.p;
-    u32 lam;
+    const pw_t p = M.p;
+    pw_t lam;
     if (A.x == B.x) {
         if (addm(A.y, B.y, p) == 0u) return ECPt{0, 0, true};
         // tangent: (3x^2 - 20 s x + 9 s^2) / 2y
-        const u32 x2 = mmul(A.x, A.x, M);
-        u32 num = mmul(E.three, x2, M);
+        const pw_t x2 = mmul(A.x, A.x, M);
+        pw_t num = mmul(E.three, x2, M);
         num = subm(num, mmul(E.s20, A.x, M), p);
         num = addm(num, E.s9sq, p);
         lam = mmul(num, invm(addm(A.y, A.y, p), M), M);
     } else {
         lam = mmul(subm(B.y, A.y, p), invm(subm(B.x, A.x, p), M), M);
     }
-    u32 x3 = addm(mmul(lam, lam, M), E.s10, p);
+    pw_t x3 = addm(mmul(lam, lam, M), E.s10, p);
     x3 = subm(subm(x3, A.x, p), B.x, p);
-    const u32 y3 = subm(mmul(lam, subm(A.x, x3, p), M), A.y, p);
+    const pw_t y3 = subm(mmul(lam, subm(A.x, x3, p), M), A.y, p);
     return ECPt{x3, y3, false};
 }
 
@@ -77,26 +79,29 @@ __device__ __forceinline__ u32 isqrt64d(u64 n) {
     return (u32)x;
 }
 
-__device__ __forceinline__ int chi(u32 a, const Mont &M) {   // a plain, a < p
+__device__ __forceinline__ int chi(pw_t a, const Mont &M) {   // a plain, a < p
     if (a == 0u) return 0;
-    const u32 v = mpow(to_mont(a, M), (M.p - 1u) / 2u, M);
+    const pw_t v = mpow(to_mont(a, M), (M.p - 1u) / 2u, M);
     return v == M.one ? 1 : -1;
 }
 
 // square root of a Montgomery quadratic residue (Tonelli-Shanks); nr is a
 // Montgomery non-residue
-__device__ u32 sqrt_m(u32 a, u32 nr, const Mont &M) {
-    const u32 p = M.p;
+__device__ pw_t sqrt_m(pw_t a, pw_t nr, const Mont &M) {
+    const pw_t p = M.p;
     if (a == 0u) return 0u;
     if ((p & 3u) == 3u) return mpow(a, (p + 1u) / 4u, M);
-    u32 q = p - 1u, S = 0;
+    pw_t q = p - 1u;
+    u32 S = 0;
     while (!(q & 1u)) { q >>= 1; ++S; }
-    u32 c = mpow(nr, q, M), x = mpow(a, (q + 1u) / 2u, M), t = mpow(a, q, M), m = S;
+    pw_t c = mpow(nr, q, M), x = mpow(a, (q + 1u) / 2u, M), t = mpow(a, q, M);
+    u32 m = S;
     for (int guard = 0; guard < 40 && t != M.one; ++guard) {
-        u32 i = 1, v = mmul(t, t, M);
+        u32 i = 1;
+        pw_t v = mmul(t, t, M);
         while (v != M.one && i < m) { v = mmul(v, v, M); ++i; }
-        if (i >= m) return 0xFFFFFFFFu;
-        u32 b = c;
+        if (i >= m) return NO_ROOT;
+        pw_t b = c;
         for (u32 k = 0; k + i + 1u < m; ++k) b = mmul(b, b, M);
         x = mmul(x, b, M);
         c = mmul(b, b, M);
@@ -110,37 +115,37 @@ __device__ __forceinline__ u64 gcd64d(u64 a, u64 b) { while (b) { u64 t = a % b;
 
 __global__ void __launch_bounds__(A4_WARPS * 32)
 a4_kernel(const PrimeDesc *primes, u32 n, u32 *out, u32 *err) {
-    __shared__ u32 hkey[A4_WARPS][A4_SLOTS];
-    __shared__ u32 hy[A4_WARPS][A4_SLOTS];
+    __shared__ pw_t hkey[A4_WARPS][A4_SLOTS];
+    __shared__ pw_t hy[A4_WARPS][A4_SLOTS];
     __shared__ unsigned short hj[A4_WARPS][A4_SLOTS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u32 idx = blockIdx.x * A4_WARPS + warp;
     if (idx >= n) return;
-    const u32 p = primes[idx].p;
+    const pw_t p = primes[idx].p;
     if (p <= 3u) { if (lane == 0) out[idx] = 0u; return; }
     const Mont M = make_mont(p);
     if (p < 1000u) {
         // direct count, characters by Euler's criterion
         u32 cnt = 0;
         for (u32 x = 1u + lane; x + 3u < p; x += 32u) {
-            const int c0 = chi(x, M);
-            cnt += (chi(x + 1u, M) == c0 && chi(x + 2u, M) == c0 && chi(x + 3u, M) == c0);
+            const int c0 = chi((pw_t)x, M);
+            cnt += (chi((pw_t)x + 1u, M) == c0 && chi((pw_t)x + 2u, M) == c0 && chi((pw_t)x + 3u, M) == c0);
         }
         cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
         if (lane == 0) out[idx] = cnt;
         return;
     }
-    u32 *keys = hkey[warp];
-    u32 *ys = hy[warp];
+    pw_t *keys = hkey[warp];
+    pw_t *ys = hy[warp];
     unsigned short *js = hj[warp];
     // least quadratic non-residue (twist parameter and Tonelli-Shanks)
     u32 nr = 0;
     for (u32 base = 2; nr == 0u && base < 100000u; base += 32u) {
-        const bool q = chi(base + lane, M) == -1;
+        const bool q = chi((pw_t)(base + lane), M) == -1;
         const u32 bal = __ballot_sync(0xFFFFFFFFu, q);
         if (bal) nr = base + (u32)(__ffs(bal) - 1);
     }
-    const u32 nrm = to_mont(nr, M);
+    const pw_t nrm = to_mont((pw_t)nr, M);
     const u32 R = isqrt64d(4ull * p);
     const u64 L = (u64)p + 1u - R, H = (u64)p + 1u + R, W = H - L;
     u32 m = isqrt64d(W + 1u);
@@ -150,30 +155,30 @@ a4_kernel(const PrimeDesc *primes, u32 n, u32 *out, u32 *err) {
     u64 N = 0;
     for (u32 attempt = 0; attempt < A4_MAX_ATTEMPTS && N == 0; ++attempt) {
         const u32 cv = attempt & 1u;
-        const u32 s = cv ? nr : 1u;
+        const pw_t s = cv ? nr : 1u;
         Curve E;
         E.M = M;
-        const u32 sm = to_mont(s, M);
-        E.s10 = mmul(to_mont(10u, M), sm, M);
-        E.s20 = mmul(to_mont(20u, M), sm, M);
-        E.s9sq = mmul(to_mont(9u, M), mmul(sm, sm, M), M);
-        E.three = to_mont(3u, M);
-        const u32 s9 = mmul(to_mont(9u, M), sm, M);
+        const pw_t sm = to_mont(s, M);
+        E.s10 = mmul(to_mont((pw_t)10, M), sm, M);
+        E.s20 = mmul(to_mont((pw_t)20, M), sm, M);
+        E.s9sq = mmul(to_mont((pw_t)9, M), mmul(sm, sm, M), M);
+        E.three = to_mont((pw_t)3, M);
+        const pw_t s9 = mmul(to_mont((pw_t)9, M), sm, M);
         // a point with y != 0: first lane whose x gives a nonzero square
         ECPt P{0, 0, true};
         for (int g = 0; g < 4096 && P.inf; ++g) {
-            const u32 xp = (nextx[cv] + lane) % p;
-            const u32 xm = to_mont(xp, M);
-            const u32 rhs = mmul(mmul(xm, subm(xm, sm, p), M), subm(xm, s9, p), M);
+            const pw_t xp = (pw_t)(nextx[cv] + lane) % p;
+            const pw_t xm = to_mont(xp, M);
+            const pw_t rhs = mmul(mmul(xm, subm(xm, sm, p), M), subm(xm, s9, p), M);
             const bool ok = rhs != 0u && mpow(rhs, (p - 1u) / 2u, M) == M.one;
             const u32 bal = __ballot_sync(0xFFFFFFFFu, ok);
             if (bal) {
                 const int f = __ffs(bal) - 1;
-                const u32 xs = __shfl_sync(0xFFFFFFFFu, xm, f);
-                const u32 rs = __shfl_sync(0xFFFFFFFFu, rhs, f);
-                const u32 y = sqrt_m(rs, nrm, M);
+                const pw_t xs = __shfl_sync(0xFFFFFFFFu, xm, f);
+                const pw_t rs = __shfl_sync(0xFFFFFFFFu, rhs, f);
+                const pw_t y = sqrt_m(rs, nrm, M);
                 nextx[cv] += (u32)f + 1u;
-                if (y != 0xFFFFFFFFu) P = ECPt{xs, y, false};
+                if (y != NO_ROOT) P = ECPt{xs, y, false};
             } else {
                 nextx[cv] += 32u;
             }
@@ -188,10 +193,10 @@ a4_kernel(const PrimeDesc *primes, u32 n, u32 *out, u32 *err) {
             ECPt Q = ec_mul(P, j0, E);
             for (u32 j = j0; j < j0 + per && j < m; ++j) {
                 if (!Q.inf) {
-                    const u32 key = Q.x + 1u;
+                    const pw_t key = Q.x + 1u;
                     u32 h = hash_slot(key, 10);
                     for (u32 probe = 0; probe < A4_SLOTS; ++probe) {
-                        const u32 old = atomicCAS(&keys[h], 0u, key);
+                        const pw_t old = cas_key(&keys[h], (pw_t)0, key);
                         if (old == 0u) { ys[h] = Q.y; js[h] = (unsigned short)j; break; }
                         if (old == key) break;
                         h = (h + 1u) & (A4_SLOTS - 1u);
@@ -211,9 +216,9 @@ a4_kernel(const PrimeDesc *primes, u32 n, u32 *out, u32 *err) {
             const u64 base = L + i * m;
             if (G.inf) { if (base <= H) found = min(found, base); }
             else {
-                u32 h = hash_slot(G.x + 1u, 10);
+                u32 h = hash_slot((pw_t)(G.x + 1u), 10);
                 for (u32 probe = 0; probe < A4_SLOTS; ++probe) {
-                    const u32 k = keys[h];
+                    const pw_t k = keys[h];
                     if (k == 0u) break;
                     if (k == G.x + 1u) {
                         const u32 j = js[h];
@@ -297,11 +302,12 @@ a4_kernel(const PrimeDesc *primes, u32 n, u32 *out, u32 *err) {
     }
     if (lane == 0) {
         if (N == 0) { atomicOr(err, 1u); out[idx] = 0u; return; }
-        const int b = 4 * chi(2u, M) + 2 * chi(6u % p, M) + 2 * chi(3u, M) + 2 * chi(p - 1u, M) + 2 * chi(p - 2u, M);
+        const int b = 4 * chi((pw_t)2, M) + 2 * chi((pw_t)6 % p, M) + 2 * chi((pw_t)3, M) + 2 * chi(p - 1u, M) +
+                      2 * chi(p - 2u, M);
         const long long num = (long long)N - 12 - b;
         if (num < 0 || (num & 7)) { atomicOr(err, 2u); out[idx] = 0u; return; }
         out[idx] = (u32)(num / 8);
     }
 }
 
-}  // namespace cz
+}  // namespace CZ_NS

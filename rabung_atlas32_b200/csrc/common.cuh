@@ -1,11 +1,20 @@
-// common.cuh -- shared types and 32-bit Montgomery arithmetic for the
-// B200 (sm_100a) census kernels.
+// common.cuh -- shared types and Montgomery arithmetic for the B200 (sm_100a)
+// census kernels.
 //
-// Montgomery product with R = 2^32 for an odd modulus p < 2^32
-// (the reference's kit::mont, src/census/engine32/src/mont32.hpp:9-10):
-//   a*b*R^-1 mod p, formed from the two high products and the carry of the
-//   low half (lo(t) + lo(m p) == 0 mod 2^32, so the carry is lo(t) != 0).
-//   Four integer multiplies (mul.lo, mul.hi, mul.lo, mul.hi) per product.
+// The kernels are compiled for one prime word width per translation unit:
+//   CZ_WIDE 0 (default): p < 2^32, pw_t = uint32_t, namespace cz;
+//   CZ_WIDE 1:           p < 2^33, pw_t = uint64_t, namespace cz64.
+// Only quantities of the size of p (p itself, residues, exponents, roots)
+// take pw_t; table numerators, run lengths, labels and canonical witnesses
+// (at most (p-1)/2 < 2^32) stay 32-bit in both.
+//
+// Montgomery product for an odd modulus p, R = 2^32 (32-bit words; the
+// reference's kit::mont, src/census/engine32/src/mont32.hpp:9-10) or R = 2^64
+// (64-bit words, p < 2^33; the reference's wide33::mont,
+// src/census/math33.hpp:13-28): a*b*R^-1 mod p, formed from the two high
+// products and the carry of the low half (lo(t) + lo(m p) == 0 mod R, so the
+// carry is lo(t) != 0).  Four integer multiplies (mul.lo, mul.hi, mul.lo,
+// mul.hi) of the word width per product.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -17,37 +26,74 @@ typedef int32_t i32;
 
 #define CZ_HD __host__ __device__ __forceinline__
 
-namespace cz {
+#ifndef CZ_WIDE
+#define CZ_WIDE 0
+#endif
+#if CZ_WIDE
+#define CZ_NS cz64
+#else
+#define CZ_NS cz
+#endif
+
+namespace CZ_NS {
+
+#if CZ_WIDE
+typedef u64 pw_t;                   // prime-sized word: p < 2^33
+#else
+typedef u32 pw_t;                   // prime-sized word: p < 2^32
+#endif
 
 struct Mont {
-    u32 p;      // odd modulus
-    u32 ninv;   // -p^-1 mod 2^32
-    u32 one;    // R mod p
-    u32 r2;     // R^2 mod p
+    pw_t p;      // odd modulus
+    pw_t ninv;   // -p^-1 mod R
+    pw_t one;    // R mod p
+    pw_t r2;     // R^2 mod p
 };
 
-CZ_HD u32 neg_inverse32(u32 p) {
-    u32 x = p;                      // p*p == 1 mod 8
-    for (int i = 0; i < 5; ++i) x *= 2u - p * x;
-    return 0u - x;
+// -p^-1 mod R by Newton steps (p*p == 1 mod 8; each step doubles the bits: 3 -> 96)
+CZ_HD pw_t neg_inverse(pw_t p) {
+    pw_t x = p;
+    for (int i = 0; i < 5; ++i) x *= (pw_t)2 - p * x;
+    return (pw_t)0 - x;
 }
 
-CZ_HD Mont make_mont(u32 p) {
+CZ_HD Mont make_mont(pw_t p) {
     Mont m;
     m.p = p;
-    m.ninv = neg_inverse32(p);
+    m.ninv = neg_inverse(p);
+#if CZ_WIDE
+    u64 R = (0ull - p) % p;                     // 2^64 mod p
+    u64 r2 = R;
+    for (int i = 0; i < 64; ++i) { r2 <<= 1; if (r2 >= p) r2 -= p; }   // 2^128 mod p (p < 2^33: no overflow)
+    m.one = R;
+    m.r2 = r2;
+#else
     u64 R = (u64(1) << 32) % p;
     m.one = (u32)R;
     m.r2 = (u32)((R * R) % p);
+#endif
     return m;
 }
 
 #ifdef __CUDA_ARCH__
 CZ_HD u32 umulhi(u32 a, u32 b) { return __umulhi(a, b); }
+CZ_HD u64 umulhi(u64 a, u64 b) { return __umul64hi(a, b); }
 #else
 CZ_HD u32 umulhi(u32 a, u32 b) { return (u32)(((u64)a * b) >> 32); }
+CZ_HD u64 umulhi(u64 a, u64 b) { return (u64)(((unsigned __int128)a * b) >> 64); }
 #endif
 
+#if CZ_WIDE
+// a*b*2^-64 mod p for a, b < p < 2^33: hi + mhi + carry < 2p, no overflow
+CZ_HD u64 mmul(u64 a, u64 b, u64 p, u64 ninv) {
+    const u64 tlo = a * b;
+    const u64 thi = umulhi(a, b);
+    const u64 m = tlo * ninv;
+    const u64 mhi = umulhi(m, p);
+    const u64 u = thi + mhi + (tlo != 0ull);
+    return u >= p ? u - p : u;
+}
+#else
 // a*b*2^-32 mod p for a, b < p
 CZ_HD u32 mmul(u32 a, u32 b, u32 p, u32 ninv) {
     u32 tlo = a * b;
@@ -57,30 +103,38 @@ CZ_HD u32 mmul(u32 a, u32 b, u32 p, u32 ninv) {
     u64 u = (u64)thi + mhi + (tlo != 0u);
     return u >= p ? (u32)(u - p) : (u32)u;
 }
+#endif
 
-CZ_HD u32 mmul(u32 a, u32 b, const Mont &M) { return mmul(a, b, M.p, M.ninv); }
-CZ_HD u32 to_mont(u32 x, const Mont &M) { return mmul(x, M.r2, M); }
-CZ_HD u32 from_mont(u32 x, const Mont &M) { return mmul(x, 1u, M); }
+CZ_HD pw_t mmul(pw_t a, pw_t b, const Mont &M) { return mmul(a, b, M.p, M.ninv); }
+CZ_HD pw_t to_mont(pw_t x, const Mont &M) { return mmul(x, M.r2, M); }
+CZ_HD pw_t from_mont(pw_t x, const Mont &M) { return mmul(x, (pw_t)1, M); }
+
+CZ_HD int top_bit(u32 e) {
+#ifdef __CUDA_ARCH__
+    return 31 - __clz(e);
+#else
+    return 31 - __builtin_clz(e);
+#endif
+}
+CZ_HD int top_bit(u64 e) {
+#ifdef __CUDA_ARCH__
+    return 63 - __clzll((long long)e);
+#else
+    return 63 - __builtin_clzll(e);
+#endif
+}
 
 // left-to-right binary power of a Montgomery residue
-CZ_HD u32 mpow(u32 a, u32 e, const Mont &M) {
+CZ_HD pw_t mpow(pw_t a, pw_t e, const Mont &M) {
     if (e == 0) return M.one;
-    int top = 31;
-#ifdef __CUDA_ARCH__
-    top = 31 - __clz(e);
-#else
-    while (!((e >> top) & 1u)) --top;
-#endif
-    u32 v = a;
+    const int top = top_bit(e);
+    pw_t v = a;
     for (int i = top - 1; i >= 0; --i) {
         v = mmul(v, v, M);
         if ((e >> i) & 1u) v = mmul(v, a, M);
     }
     return v;
 }
-
-// plain modular helpers (64-bit, host or device, setup only)
-CZ_HD u32 mulmod64(u32 a, u32 b, u32 p) { return (u32)(((u64)a * b) % p); }
 
 CZ_HD u32 gcd32(u32 a, u32 b) {
     while (b) { u32 t = a % b; a = b; b = t; }
@@ -94,7 +148,7 @@ CZ_HD u32 lcm_of_mask(u32 mask) {
     return m;
 }
 
-CZ_HD u32 mask_of(u32 p) {
+CZ_HD u32 mask_of(pw_t p) {
     u32 m = 0;
     for (u32 r = 2; r <= 9; ++r)
         if ((p - 1u) % r == 0u) m |= 1u << (r - 2);
@@ -112,12 +166,12 @@ CZ_HD u32 key_witness(u64 k) { return 0xFFFFFFFFu - (u32)k; }
 // ---- per-prime and per-profile descriptors shared by host and device ----
 
 struct PrimeDesc {
-    u32 p;
+    pw_t p;
     u32 mask;
     u32 m;           // lcm of admissible r
-    u32 e;           // (p-1)/m
-    u32 ninv, one, r2;
-    u32 z;           // Montgomery form of an element of exact order m
+    pw_t e;          // (p-1)/m
+    pw_t ninv, one, r2;
+    pw_t z;          // Montgomery form of an element of exact order m
     u32 sigma;       // label of -1 modulo m (0 or m/2)
     u32 B;           // signed table radius (sparse)
     u32 K0;          // base view: index of n is n + 32*K0 + 31
@@ -139,7 +193,7 @@ struct ProfDesc {
     u32 D;           // cover denominators 1..D
     u32 out_slot;    // index in the caller's output array
     u64 plane_off;   // word offset of plane 0 in the plane pool
-    u32 omega[9];    // Montgomery omega^j, omega = z^(m/r), j < r
+    pw_t omega[9];   // Montgomery omega^j, omega = z^(m/r), j < r
     u32 local;       // index of the prime within its route's list
     u32 qspec;       // speculative threshold (0: none); exact if the best run reaches it
     u32 tpref;       // preferred anchor stages (sparse filter)
@@ -171,4 +225,4 @@ enum : u32 {
     ST_SPEC = 1u << 8,       // best run below the speculative threshold: re-run without it
 };
 
-}  // namespace cz
+}  // namespace CZ_NS

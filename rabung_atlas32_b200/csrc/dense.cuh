@@ -16,7 +16,7 @@
 #pragma once
 #include "labels.cuh"
 
-namespace cz {
+namespace CZ_NS {
 
 constexpr int DENSE_WARPS = 8;           // warps per CTA = segments per chunk
 constexpr int DENSE_STEPS = 256;         // 32-wide steps per segment
@@ -74,12 +74,12 @@ struct DenseArgs {
 // One CTA per (prime, chunk of DENSE_WARPS segments); one warp per segment.
 __global__ void __launch_bounds__(DENSE_WARPS * 32)
 dense_scan_kernel(DenseArgs a) {
-    extern __shared__ u32 dsm[];
+    extern __shared__ __align__(16) u32 dsm[];
     __shared__ Summ wsum[DENSE_WARPS][8];
     __shared__ u32 cur_prime;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     u32 prev_prime = 0xFFFFFFFFu;
-    u32 *keys = dsm;
+    pw_t *keys = reinterpret_cast<pw_t *>(dsm);
     unsigned short *labs = nullptr;
     u32 slots = 0;
     for (u32 chunk = blockIdx.x; chunk < a.nchunks; chunk += gridDim.x) {
@@ -102,7 +102,7 @@ dense_scan_kernel(DenseArgs a) {
             prev_prime = pi;
         }
         const u32 local_chunk = chunk - a.chunk_prefix[pi];
-        const u32 nh = (P.p - 1u) >> 1;
+        const u32 nh = (u32)((P.p - 1u) >> 1);             // p < 2^33: fits 32 bits
         const u32 seg = local_chunk * DENSE_WARPS + warp;
         const u32 seg_start = 1u + seg * a.seg;              // x of the first element
         const u32 nprof = P.nprof;
@@ -129,7 +129,7 @@ dense_scan_kernel(DenseArgs a) {
                 const u32 nvalid = min(32u, seg_end - base + 1u);
                 u32 label = 0;
                 if (valid) {
-                    u32 y = mpow(to_mont(x, M), P.e, M);
+                    const pw_t y = mpow(to_mont((pw_t)x, M), P.e, M);
                     label = lookup_label(keys, labs, slots, y);
                     if (label == 0xFFFFu) { bad = 1; label = 0; }
                 }
@@ -269,13 +269,14 @@ __global__ void dense_merge_kernel(DenseMergeArgs a, const u32 *dense_prof_list,
         tot = h2 ? merge_summ(tot, mine[l]) : mine[l];
         h2 = true;
     }
-    const u32 p = P.p, nh = (p - 1u) >> 1, r = D.r;
+    const pw_t p = P.p;
+    const u32 nh = (u32)((p - 1u) >> 1), r = D.r;
     const bool sym = (nh % r) == 0u;     // r | (p-1)/2: colour(p-x) = colour(x)
     u32 bl = tot.best, bs = tot.bstart;
     u32 L;
     if (tot.pre == nh) {
         // the whole half interval is one run
-        if (sym) { bl = p - 1u; bs = 1u; L = p - 1u; }
+        if (sym) { bl = (u32)(p - 1u); bs = 1u; L = (u32)(p - 1u); }
         else { bl = nh; bs = 1u; L = nh; }
     } else {
         take_best(bl, bs, tot.pre, 1u);                       // run from x = 1
@@ -287,4 +288,4 @@ __global__ void dense_merge_kernel(DenseMergeArgs a, const u32 *dense_prof_list,
     a.prefix_out[gprof] = L;
 }
 
-}  // namespace cz
+}  // namespace CZ_NS

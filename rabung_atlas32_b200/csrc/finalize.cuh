@@ -12,11 +12,11 @@
 #pragma once
 #include "labels.cuh"
 
-namespace cz {
+namespace CZ_NS {
 
-// deterministic Miller-Rabin for n < 2^32 with bases 2, 3, 5, 7, 11 (no strong
-// pseudoprime to all five below 2.15e12)
-__device__ inline bool is_prime32(u32 n) {
+// deterministic Miller-Rabin with bases 2, 3, 5, 7, 11: no strong pseudoprime
+// to all five below 2.15e12, so exact for every n < 2^33
+__device__ inline bool is_prime_word(pw_t n) {
     if (n < 2u) return false;
     const u32 bases[5] = {2, 3, 5, 7, 11};
     for (int i = 0; i < 5; ++i) {
@@ -24,11 +24,12 @@ __device__ inline bool is_prime32(u32 n) {
         if (n % bases[i] == 0u) return false;
     }
     const Mont M = make_mont(n);
-    u32 d = n - 1u, s = 0;
+    pw_t d = n - 1u;
+    u32 s = 0;
     while (!(d & 1u)) { d >>= 1; ++s; }
-    const u32 mone = n - M.one;           // Montgomery form of -1
+    const pw_t mone = n - M.one;          // Montgomery form of -1
     for (int i = 0; i < 5; ++i) {
-        u32 x = mpow(to_mont(bases[i], M), d, M);
+        pw_t x = mpow(to_mont((pw_t)bases[i], M), d, M);
         if (x == M.one || x == mone) continue;
         bool pass = false;
         for (u32 j = 1; j < s; ++j) {
@@ -46,7 +47,7 @@ __global__ void setup_kernel(PrimeDesc *primes, ProfDesc *profs, ProfState *stat
     if (i >= n) return;
     PrimeDesc P = primes[i];
     u32 status = 0;
-    if (!is_prime32(P.p)) status |= ST_ROOT;
+    if (!is_prime_word(P.p)) status |= ST_ROOT;
     if (P.p > 2u) {
         const Mont M = make_mont(P.p);
         P.ninv = M.ninv; P.one = M.one; P.r2 = M.r2;
@@ -59,8 +60,8 @@ __global__ void setup_kernel(PrimeDesc *primes, ProfDesc *profs, ProfState *stat
         P.sigma = (P.e & 1u) ? P.m / 2u : 0u;
         for (u32 s = 0; s < P.nprof; ++s) {
             ProfDesc &D = profs[P.first_prof + s];
-            const u32 w = mpow(P.z, P.m / D.r, M);
-            u32 v = M.one;
+            const pw_t w = mpow(P.z, (pw_t)(P.m / D.r), M);
+            pw_t v = M.one;
             for (u32 j = 0; j < 9; ++j) {
                 D.omega[j] = j < D.r ? v : 0u;
                 v = mmul(v, w, M);
@@ -74,13 +75,19 @@ __global__ void setup_kernel(PrimeDesc *primes, ProfDesc *profs, ProfState *stat
     primes[i] = P;
 }
 
-struct OutRecord {      // mirrors cz_profile in include/rabung_census.h
-    u32 p, r, M, L, witness, status;
+// mirrors cz_profile (32-bit words) or cz_profile64 (64-bit words) in
+// include/rabung_census.h; the canonical witness is at most (p-1)/2 < 2^32
+struct OutRecord {
+    pw_t p;
+    u32 r, M, L, witness, status;
+#if CZ_WIDE
+    u32 reserved;
+#endif
     unsigned long long K;
 };
 
-__device__ __forceinline__ u32 colour_pow(u32 x, const Mont &M, u32 ex, const u32 *om, u32 r) {
-    const u32 y = mpow(to_mont(x, M), ex, M);
+__device__ __forceinline__ u32 colour_pow(pw_t x, const Mont &M, pw_t ex, const pw_t *om, u32 r) {
+    const pw_t y = mpow(to_mont(x, M), ex, M);
     for (u32 j = 0; j < r; ++j)
         if (om[j] == y) return j;
     return 0xFFFFFFFFu;
@@ -94,7 +101,8 @@ __global__ void finalize_kernel(const PrimeDesc *primes, const ProfDesc *profs, 
     const PrimeDesc P = primes[D.prime];
     const ProfState S = state[g];
     const Mont M{P.p, P.ninv, P.one, P.r2};
-    const u32 p = P.p, r = D.r, ex = (p - 1u) / r;
+    const pw_t p = P.p, ex = (p - 1u) / D.r;
+    const u32 r = D.r;
     u32 status = P.status | S.status;
     const u32 Mlen = key_len(S.best), w = key_witness(S.best);
     if (S.best == 0ull && !(D.qspec && P.route == 2u)) status |= ST_VERIFY;
@@ -104,30 +112,34 @@ __global__ void finalize_kernel(const PrimeDesc *primes, const ProfDesc *profs, 
         L = dense_prefix[g];
     } else {
         L = 1;                                   // colour(1) = 0
-        while (L + 1u < p && colour_pow(L + 1u, M, ex, D.omega, r) == 0u) {
+        while (L + 1u < p && colour_pow((pw_t)L + 1u, M, ex, D.omega, r) == 0u) {
             ++L;
             if (L > 4096u) { status |= ST_PREFIX; break; }
         }
     }
     if (verify && !(status & (ST_ROOT | ST_LABEL)) && Mlen > 0u && Mlen <= 4096u) {
         // the run [w, w+M-1] (or its mirror) is monochromatic and maximal
-        const u32 c0 = colour_pow(w, M, ex, D.omega, r);
-        bool ok = c0 != 0xFFFFFFFFu && (u64)w + Mlen - 1u <= p - 1u;
-        for (u32 k = 1; ok && k < Mlen; ++k) ok = colour_pow(w + k, M, ex, D.omega, r) == c0;
-        if (ok && w > 1u) ok = colour_pow(w - 1u, M, ex, D.omega, r) != c0;
-        if (ok && (u64)w + Mlen <= p - 1u) ok = colour_pow(w + Mlen, M, ex, D.omega, r) != c0;
+        const pw_t wx = w;
+        const u32 c0 = colour_pow(wx, M, ex, D.omega, r);
+        bool ok = c0 != 0xFFFFFFFFu && (u64)w + Mlen - 1u <= (u64)p - 1u;
+        for (u32 k = 1; ok && k < Mlen; ++k) ok = colour_pow(wx + k, M, ex, D.omega, r) == c0;
+        if (ok && w > 1u) ok = colour_pow(wx - 1u, M, ex, D.omega, r) != c0;
+        if (ok && (u64)w + Mlen <= (u64)p - 1u) ok = colour_pow(wx + Mlen, M, ex, D.omega, r) != c0;
         u32 pl = 1;                              // prefix re-check from the scan result
         if (ok && P.route == 1u) {
-            while (pl + 1u < p && pl <= L && colour_pow(pl + 1u, M, ex, D.omega, r) == 0u) ++pl;
+            while (pl + 1u < p && pl <= L && colour_pow((pw_t)pl + 1u, M, ex, D.omega, r) == 0u) ++pl;
             ok = pl == L;
         }
         if (!ok) status |= ST_VERIFY;
     }
     OutRecord o;
     o.p = p; o.r = r; o.M = Mlen; o.L = L; o.witness = w; o.status = status;
+#if CZ_WIDE
+    o.reserved = 0u;
+#endif
     const u64 b = ((((u64)p - 1u) / 2u) % r == 0u) ? 2ull * L + 2ull : (u64)L + 2ull;
     o.K = (u64)Mlen + 1ull > b ? (u64)Mlen + 1ull : b;
     out[D.out_slot] = o;
 }
 
-}  // namespace cz
+}  // namespace CZ_NS

@@ -52,7 +52,7 @@
 #pragma once
 #include "labels.cuh"
 
-namespace cz {
+namespace CZ_NS {
 
 #ifndef CZ_SB1                       // anchor stages whose loads issue together, by stored planes
 #define CZ_SB1 5                     // r = 2 runs t - 1 = 10 stages: two batches of 5
@@ -160,11 +160,12 @@ struct View {
 };
 
 struct ProfCtx {
-    u32 p, r, np, npp, Q, D, B, NW, OFF, ex;
+    pw_t p, ex;            // prime, (p - 1) / r
+    u32 r, np, npp, Q, D, B, NW, OFF;
     Mont M;
     const u32 *P;          // base view planes
     View base, odd;
-    u32 om[9];
+    pw_t om[9];
     u32 seed, qspec;       // certified stretch from the table, speculative threshold
     u32 tpref;             // preferred anchor stages for this order
     u32 NW2;               // odd view words per plane
@@ -183,8 +184,8 @@ __device__ __forceinline__ u32 colour_at(const ProfCtx &c, u32 u) {
 }
 
 // absolute colour of x in [1, p-1] by a direct power: x^((p-1)/r) = omega^j
-__device__ __forceinline__ u32 colour_direct(u32 x, const ProfCtx &c) {
-    const u32 y = mpow(to_mont(x, c.M), c.ex, c.M);
+__device__ __forceinline__ u32 colour_direct(pw_t x, const ProfCtx &c) {
+    const pw_t y = mpow(to_mont(x, c.M), c.ex, c.M);
     for (u32 j = 0; j < c.r; ++j)
         if (c.om[j] == y) return j;
     return 0xFFFFFFFFu;
@@ -193,10 +194,10 @@ __device__ __forceinline__ u32 colour_direct(u32 x, const ProfCtx &c) {
 // exact completion of one candidate; returns packed key (0 on reject) and
 // sets *err on an arithmetic failure
 __device__ __noinline__ u64 complete_one(const ProfCtx &c, u32 b, u32 d, u32 *err) {
-    const u32 p = c.p;
+    const pw_t p = c.p;
     // Montgomery d^-1 (= R d^-1), so mmul(b, dinv) = b d^-1 mod p
-    const u32 dinv = mpow(to_mont(d, c.M), c.p - 2u, c.M);
-    const u32 xr = mmul(b, dinv, c.M);
+    const pw_t dinv = mpow(to_mont((pw_t)d, c.M), c.p - 2u, c.M);
+    const pw_t xr = mmul((pw_t)b, dinv, c.M);
     if (xr == 0u) return 0;
     const u32 cb = colour_at(c, b + c.OFF);
     const u32 cd = colour_at(c, d + c.OFF);
@@ -207,22 +208,22 @@ __device__ __noinline__ u64 complete_one(const ProfCtx &c, u32 b, u32 d, u32 *er
         const u64 x = (u64)xr + k;
         if (x >= p) break;
         const u64 n = (u64)b + (u64)k * d;
-        const bool same = n <= c.B ? colour_at(c, (u32)n + c.OFF) == cb : colour_direct((u32)x, c) == A;
+        const bool same = n <= c.B ? colour_at(c, (u32)n + c.OFF) == cb : colour_direct((pw_t)x, c) == A;
         if (!same) break;
         right = k;
     }
     for (u32 k = 1;; ++k) {                            // x = xr - k, numerator b - k d
         if (k > RUN_CAP) { *err = 1; return 0; }
         if (k >= xr) break;
-        const u32 x = xr - k;
+        const pw_t x = xr - k;
         const i64 n = (i64)b - (i64)k * d;
         const bool same = n >= -(i64)c.B ? colour_at(c, (u32)(n + (i64)c.OFF)) == cb : colour_direct(x, c) == A;
         if (!same) break;
         left = k;
     }
-    const u32 s = xr - left, e = xr + right;
-    const u32 w = s < p - e ? s : p - e;
-    return pack_key(e - s + 1u, w);
+    const pw_t s = xr - left, e = xr + right;
+    const pw_t w = s < p - e ? s : p - e;             // canonical witness: at most (p - 1) / 2 < 2^32
+    return pack_key((u32)(e - s + 1u), (u32)w);
 }
 
 // bilateral screen of one word at view index i0 (row step dd = d / G): keep
@@ -731,4 +732,4 @@ sparse_kernel(SparseArgs a) {
     }
 }
 
-}  // namespace cz
+}  // namespace CZ_NS

@@ -37,7 +37,7 @@
 #pragma once
 #include "labels.cuh"
 
-namespace cz {
+namespace CZ_NS {
 
 constexpr int TABLE_THREADS = 1024;
 constexpr int TABLE_WARPS = TABLE_THREADS / 32;
@@ -70,7 +70,7 @@ struct TabWarp {            // per-warp, per-profile carried state
 
 __global__ void __launch_bounds__(TABLE_THREADS, 1)
 table_kernel(TableArgs a) {
-    extern __shared__ u32 tsm[];
+    extern __shared__ __align__(16) u32 tsm[];
     __shared__ TabProf tp[8];
     __shared__ unsigned short lab[TABLE_WARPS][TABLE_SUB + 1][32];
     __shared__ TabWarp tw[TABLE_WARPS];
@@ -80,9 +80,11 @@ table_kernel(TableArgs a) {
         const PrimeDesc P = a.primes[pi];
         const Mont M{P.p, P.ninv, P.one, P.r2};
         const u32 slots = hash_slots(P.m);
-        u32 *keys = tsm;
+        // shared layout: root hash keys (slots words), their labels (slots u16),
+        // 4 u16 of padding, labels of the primes below the table end
+        pw_t *keys = reinterpret_cast<pw_t *>(tsm);
         unsigned short *hl = reinterpret_cast<unsigned short *>(keys + slots);
-        unsigned short *plab = reinterpret_cast<unsigned short *>(keys + slots + slots / 2u + 2u);
+        unsigned short *plab = hl + slots + 4u;
         build_root_hash(keys, hl, slots, M, P.z, P.m);
         const u32 KS = (P.B + 1u + 31u) / 32u + 1u;            // steps: n in [0, 32*KS)
         const u32 nmax = 32u * KS;
@@ -94,7 +96,7 @@ table_kernel(TableArgs a) {
         const u32 nq = lo;
         u32 bad = (nmax > a.chain_limit) ? 1u : 0u;
         for (u32 i = threadIdx.x; i < nq; i += blockDim.x) {
-            u32 y = mpow(to_mont(a.small_primes[i], M), P.e, M);
+            const pw_t y = mpow(to_mont((pw_t)a.small_primes[i], M), P.e, M);
             u32 l = lookup_label(keys, hl, slots, y);
             if (l == 0xFFFFu) { bad = 1; l = 0; }
             plab[i] = (unsigned short)l;
@@ -283,4 +285,4 @@ table_kernel(TableArgs a) {
     }
 }
 
-}  // namespace cz
+}  // namespace CZ_NS

@@ -32,7 +32,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .census import Census, CensusError, Tuning, to_records
+from .census import Census, CensusError, Tuning, config, to_records
 
 
 @dataclass
@@ -72,16 +72,7 @@ class Server:
         self.lib = _lib.load()
         probe = Census(device=device, tuning=tuning)      # resolves the tuning saved for this device
         try:
-            t = probe.tuning
-            cfg = _lib.cz_config()
-            self.lib.cz_default_config(ctypes.byref(cfg))
-            cfg.device = device
-            cfg.sparse_min_p, cfg.cover_n, cfg.anchor_bits, cfg.screen = t.sparse_min_p, t.cover_n, t.anchor_bits, t.screen
-            cfg.sparse_blocks, cfg.use_graph, cfg.cta_per_profile = t.sparse_blocks, t.use_graph, t.cta_per_profile
-            cfg.epoch_rows, cfg.speculate, cfg.plane_budget_mb = t.epoch_rows, t.speculate, t.plane_budget_mb
-            cfg.dense_steps = t.dense_steps
-            for r in range(10):
-                cfg.q_cap[r], cfg.spec_margin10[r], cfg.anchor_t[r] = t.q_cap[r], t.spec_margin10[r], t.anchor_t[r]
+            cfg = config(self.lib, device, probe.tuning)
         finally:
             probe.close()
         h = ctypes.c_void_p()

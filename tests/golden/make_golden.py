@@ -28,6 +28,14 @@ Writes into tests/golden/:
   refcpu_2p24.json.gz -- `independent p r 3` (full-walk reference) on a seeded
                         sample of (p, r) pairs from the 4096 primes from 2^24,
                         and moment_worker A4 for all 4096 of them.
+  wide33.json.gz     -- the 33-bit domain: reproducibility/gpu_method/throughput/
+                        holdout-33-mr_selected.json windows[*].profiles_full
+                        (2 x 1024 primes between 2^32 and 2^33), the reference
+                        GPU dense-oracle records with 2^32 <= p < 2^33, and A4
+                        of every holdout prime by the reference's point counter
+                        (src/census/theorie/elliptic4_mestre.cpp, `elliptic4`).
+
+`--parts wide` regenerates only wide33.json.gz.
 """
 from __future__ import annotations
 
@@ -92,15 +100,47 @@ def main():
     ap.add_argument("--ref", required=True, help="checkout of the reference repository")
     ap.add_argument("--samples", type=int, default=48, help="(p, r) pairs of the 2^24 block for `independent`")
     ap.add_argument("--jobs", type=int, default=8)
+    ap.add_argument("--parts", default="all", choices=["all", "wide"])
     a = ap.parse_args()
     ref = Path(a.ref)
     ref_bin = REPO / "oracle" / "_ref"
+    gm = ref / "reproducibility" / "gpu_method"
+
+    # 33-bit domain
+    hold = json.loads((gm / "throughput" / "holdout-33-mr_selected.json").read_text())
+    wins = []
+    for w in hold["windows"]:
+        rows = [[row["p"], [[v["r"], v["max"], v["prefix"], v["K"], v["witness"]] for v in row["profiles"]]]
+                for row in w["profiles_full"]]
+        wins.append({"lo": w["lo"], "hi": w["hi"], "rows": rows})
+    wide = {}
+    for rec in json.loads((gm / "night" / "ORACLES_NOUVEAUX.json").read_text()):
+        if 2 ** 32 <= rec["p"] < 2 ** 33 and rec.get("status") == "PASS":
+            wide[rec["p"]] = rec["profiles"]
+    for res in json.loads((gm / "throughput" / "CONTROLES_INDEPENDANTS.json").read_text())["results"]:
+        rec = res.get("oracle", {}).get("record", {})
+        if 2 ** 32 <= rec.get("p", 0) < 2 ** 33 and rec.get("status") == "PASS":
+            wide[rec["p"]] = rec["profiles"]
+    hp = sorted({row[0] for w in wins for row in w["rows"]})
+    a4w = {}
+    for i in range(0, len(hp), 256):
+        out = subprocess.run([str(ref_bin / "elliptic4"), *map(str, hp[i:i + 256])], capture_output=True,
+                             check=True, text=True).stdout
+        for line in out.splitlines():
+            j = json.loads(line)
+            assert j["status"] == "PASS"
+            a4w[str(j["p"])] = j["quadruples"]
+    dump("wide33.json.gz", {"holdout": wins, "a4": a4w,
+                            "dense_oracle": [[p, [[v["r"], v["max"], v["prefix"], v["K"], v["witness"]] for v in prof]]
+                                             for p, prof in sorted(wide.items())]})
+    if a.parts == "wide":
+        print("wide33.json.gz written to", HERE)
+        return
 
     for f in ["scan-00000.vdw", "quadruplets-00000.a4", "scan-49900.vdw",
               "quadruplets-49900.a4", "manifest.json"]:
         shutil.copyfile(ref / "data" / "sample" / f, HERE / f)
 
-    gm = ref / "reproducibility" / "gpu_method"
     hold = json.loads((gm / "throughput" / "holdout-32-mr_selected.json").read_text())
     windows = []
     for w in hold["windows"]:

@@ -56,3 +56,15 @@ def test_default_config_and_bad_tuning_refused_before_device():
     lib.cz_default_config(ctypes.byref(cfg))
     cfg.cover_n = 1
     assert lib.cz_open(ctypes.byref(cfg), ctypes.byref(h)) == _lib.CZ_EINVAL
+
+
+def test_count_profiles64_host_only():
+    """The wide count needs no GPU; primes at or above 2^33 give 0."""
+    from rabung_atlas32_b200 import _lib, codec
+    lib = _lib.load()
+    ps = [3, 4294967311, 5389000007, 8589934583]
+    arr = (ctypes.c_uint64 * len(ps))(*ps)
+    assert lib.cz_count_profiles64(arr, len(ps)) == sum(bin(codec.expected_mask(p)).count("1") for p in ps)
+    big = (ctypes.c_uint64 * 1)(2 ** 33 + 17)
+    assert lib.cz_count_profiles64(big, 1) == 0
+    assert ctypes.sizeof(_lib.cz_profile64) == 40

@@ -333,12 +333,14 @@ def main(argv=None):
 
         python -m rabung_atlas32_b200.census --ending 4294967291 --count 512 --mode sparse
         python -m rabung_atlas32_b200.census --from 16777216 --count 4096 --mode dense --a4
+        python -m rabung_atlas32_b200.census --microbench        (measured integer peaks)
     """
     import argparse
     import json
     from . import sieve
     ap = argparse.ArgumentParser(description=main.__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     g = ap.add_mutually_exclusive_group(required=True)
+    g.add_argument("--microbench", action="store_true", help="print this GPU's measured integer peaks")
     g.add_argument("--ending", type=int, help="the window ends at this prime")
     g.add_argument("--from", dest="start", type=int, help="the window starts at the first prime >= this")
     ap.add_argument("--count", type=int, default=4096)
@@ -346,6 +348,10 @@ def main(argv=None):
     ap.add_argument("--a4", action="store_true")
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args(argv)
+    if a.microbench:
+        with Census() as c:
+            print(json.dumps({"plane_word_tests_per_s": c.microbench(0), "montgomery_products_per_s": c.microbench(1)}))
+        return
     ps = sieve.primes_ending(a.ending, a.count) if a.ending else sieve.primes_from(a.start, a.count)
     with Census() as c:
         for _ in range(a.repeat):

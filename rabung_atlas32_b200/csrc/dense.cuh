@@ -58,6 +58,14 @@ __device__ __forceinline__ Summ merge_summ(const Summ &a, const Summ &b) {
     return o;
 }
 
+// warp-uniform run state of one profile within a warp's segment
+struct DRun {
+    u32 r, mg;                   // order, its division magic
+    u32 carry_c, carry_start, carry_len;   // colour, start and length of the run open at the last x
+    u32 pre, bl, bs, cf, inpre;  // prefix run, best closed run (length, start), first colour, prefix open
+    u32 pad[2];
+};
+
 struct DenseArgs {
     const PrimeDesc *primes;       // all primes of the call
     const u32 *dense_idx;          // dense-local index -> prime index
@@ -76,6 +84,7 @@ __global__ void __launch_bounds__(DENSE_WARPS * 32)
 dense_scan_kernel(DenseArgs a) {
     extern __shared__ __align__(16) u32 dsm[];
     __shared__ Summ wsum[DENSE_WARPS][8];
+    __shared__ __align__(16) DRun drun[DENSE_WARPS][8];
     __shared__ u32 cur_prime;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     u32 prev_prime = 0xFFFFFFFFu;
@@ -106,19 +115,16 @@ dense_scan_kernel(DenseArgs a) {
         const u32 seg = local_chunk * DENSE_WARPS + warp;
         const u32 seg_start = 1u + seg * a.seg;              // x of the first element
         const u32 nprof = P.nprof;
-        // per-profile warp-uniform state
-        u32 rr[8], mg[8], carry_c[8], carry_start[8], carry_len[8], pre[8], bl[8], bs[8], cf[8];
-        bool inpre[8];
-#pragma unroll
-        for (int s = 0; s < 8; ++s) {
-            u32 r = s < (int)nprof ? a.profs[P.first_prof + s].r : 2u;
-            rr[s] = r; mg[s] = magic_of(r);
-            carry_c[s] = 0xFFFFFFFFu; carry_start[s] = seg_start; carry_len[s] = 0;
-            pre[s] = 0; bl[s] = 0; bs[s] = 0; cf[s] = 0; inpre[s] = true;
+        // per-profile run state: warp-uniform, so it lives in this warp's shared
+        // records (one read and one write per profile per 32 x) instead of
+        // registers, which keeps the kernel's occupancy up
+        if ((u32)lane < nprof) {
+            const u32 r = a.profs[P.first_prof + lane].r;
+            drun[warp][lane] = DRun{r, magic_of(r), 0xFFFFFFFFu, seg_start, 0u, 0u, 0u, 0u, 0u, 1u, 0u, 0u};
         }
-        u32 lastc[8];
-        bool active = seg_start <= nh;
-        u32 seg_end = active ? min(nh, seg_start + a.seg - 1u) : 0u;   // inclusive
+        __syncwarp();
+        const bool active = seg_start <= nh;
+        const u32 seg_end = active ? min(nh, seg_start + a.seg - 1u) : 0u;   // inclusive
         u32 bad = 0;
         if (active) {
             const u32 nsteps = (seg_end - seg_start) / 32u + 1u;
@@ -133,15 +139,14 @@ dense_scan_kernel(DenseArgs a) {
                     label = lookup_label(keys, labs, slots, y);
                     if (label == 0xFFFFu) { bad = 1; label = 0; }
                 }
-#pragma unroll
-                for (int s = 0; s < 8; ++s) {
-                    if (s >= (int)nprof) break;
-                    const u32 c = mod_small(label, rr[s], mg[s]);
+                for (u32 s = 0; s < nprof; ++s) {
+                    DRun R = drun[warp][s];
+                    const u32 c = mod_small(label, R.r, R.mg);
                     u32 pc = __shfl_up_sync(0xFFFFFFFFu, c, 1);
-                    if (lane == 0) pc = carry_c[s];
+                    if (lane == 0) pc = R.carry_c;
                     const bool chg = valid && (c != pc);
                     const u32 C = __ballot_sync(0xFFFFFFFFu, chg);
-                    if (st == 0) cf[s] = __shfl_sync(0xFFFFFFFFu, c, 0);
+                    if (st == 0) R.cf = __shfl_sync(0xFFFFFFFFu, c, 0);
                     // run closing at lane-1 for each lane that starts a new run
                     u32 clen = 0, cst = 0;
                     if (chg) {
@@ -150,16 +155,16 @@ dense_scan_kernel(DenseArgs a) {
                             const u32 h = 31u - __clz(below);
                             clen = lane - h; cst = base + h;
                         } else {
-                            clen = carry_len[s] + lane; cst = carry_start[s];
+                            clen = R.carry_len + lane; cst = R.carry_start;
                         }
                     }
                     // the first closed run of the segment is its prefix run
-                    if (inpre[s] && C) {
+                    if (R.inpre && C) {
                         const u32 first = __ffs(C) - 1u;   // lowest change lane
                         const u32 plen = __shfl_sync(0xFFFFFFFFu, clen, first);
                         if (plen > 0) {
-                            pre[s] = plen;
-                            inpre[s] = false;
+                            R.pre = plen;
+                            R.inpre = 0u;
                             if (lane == (int)first) clen = 0;
                         } else {
                             // change at the segment's first element: the empty carry run
@@ -167,42 +172,43 @@ dense_scan_kernel(DenseArgs a) {
                             if (rest) {
                                 const u32 f2 = __ffs(rest) - 1u;
                                 const u32 pl2 = __shfl_sync(0xFFFFFFFFu, clen, f2);
-                                pre[s] = pl2;
-                                inpre[s] = false;
+                                R.pre = pl2;
+                                R.inpre = 0u;
                                 if (lane == (int)f2) clen = 0;
                             }
                         }
                     }
                     const u32 mlen = __reduce_max_sync(0xFFFFFFFFu, clen);
-                    if (mlen > 0 && mlen >= bl[s]) {
+                    if (mlen > 0 && mlen >= R.bl) {
                         const u32 mst = __reduce_min_sync(0xFFFFFFFFu, clen == mlen ? cst : 0xFFFFFFFFu);
-                        take_best(bl[s], bs[s], mlen, mst);
+                        take_best(R.bl, R.bs, mlen, mst);
                     }
                     if (C) {
                         const u32 h = 31u - __clz(C);
-                        carry_start[s] = base + h;
-                        carry_len[s] = nvalid - h;
+                        R.carry_start = base + h;
+                        R.carry_len = nvalid - h;
                     } else {
-                        carry_len[s] += nvalid;
+                        R.carry_len += nvalid;
                     }
-                    carry_c[s] = __shfl_sync(0xFFFFFFFFu, c, nvalid - 1u);
-                    lastc[s] = carry_c[s];
+                    R.carry_c = __shfl_sync(0xFFFFFFFFu, c, nvalid - 1u);
+                    __syncwarp();
+                    drun[warp][s] = R;                     // every lane writes the same record
+                    __syncwarp();
                 }
             }
         }
         bad = __reduce_or_sync(0xFFFFFFFFu, bad);
         if (lane == 0) {
             if (bad) atomicOr(&a.state[P.first_prof].status, ST_LABEL);
-#pragma unroll
-            for (int s = 0; s < 8; ++s) {
-                if (s >= (int)nprof) break;
+            for (u32 s = 0; s < nprof; ++s) {
+                const DRun &R = drun[warp][s];
                 Summ o;
                 if (active) {
                     o.start = seg_start; o.len = seg_end - seg_start + 1u;
-                    o.suf = carry_len[s];
-                    o.pre = inpre[s] ? o.len : pre[s];
-                    o.best = bl[s]; o.bstart = bs[s];
-                    o.cf = cf[s]; o.cl = lastc[s];
+                    o.suf = R.carry_len;
+                    o.pre = R.inpre ? o.len : R.pre;
+                    o.best = R.bl; o.bstart = R.bs;
+                    o.cf = R.cf; o.cl = R.carry_c;
                 } else {
                     o.start = 0; o.len = 0; o.pre = o.suf = o.best = o.bstart = 0; o.cf = o.cl = 0;
                 }

@@ -197,6 +197,7 @@ struct ProfDesc {
     u32 local;       // index of the prime within its route's list
     u32 qspec;       // speculative threshold (0: none); exact if the best run reaches it
     u32 tpref;       // preferred anchor stages (sparse filter)
+    u32 req;         // serving: the request slot this profile belongs to
 };
 
 // device-written per-profile results
@@ -206,6 +207,8 @@ struct ProfState {
     u32 seed;                 // longest monochromatic stretch seen in [1, B]
     u32 firstnz;              // least n >= 1 with colour != 0 (prefix + 1)
     u32 status;
+    u32 active;               // serving: CTAs working on the profile now
+    u32 done;                 // serving: 1 once its record is final
     u32 pad;
     unsigned long long words;       // filter words visited
     unsigned long long completions; // exact completions run

@@ -412,7 +412,7 @@ int enqueue(CZ_HANDLE *h, bool timed, u32 &launches) {
     rec(2);
     if (h->nsl) {
         cudaMemsetAsync(h->b_counter.p, 0, 64, st);
-        SparseArgs sa;
+        SparseArgs sa{};                       // serving fields stay null: one-call census
         sa.primes = P<PrimeDesc>(h->b_primes);
         sa.profs = P<ProfDesc>(h->b_profs);
         sa.state = P<ProfState>(h->b_state);

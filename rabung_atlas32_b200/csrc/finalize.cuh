@@ -68,7 +68,7 @@ __global__ void setup_kernel(PrimeDesc *primes, ProfDesc *profs, ProfState *stat
             }
             ProfState &S = state[P.first_prof + s];
             S.best = 0; S.claim = 0; S.seed = 0; S.firstnz = 0xFFFFFFFFu;
-            S.status = 0; S.pad = 0; S.words = 0; S.completions = 0; S.tests = 0;
+            S.status = 0; S.active = 0; S.done = 0; S.pad = 0; S.words = 0; S.completions = 0; S.tests = 0;
         }
     }
     P.status = status;
@@ -93,19 +93,23 @@ __device__ __forceinline__ u32 colour_pow(pw_t x, const Mont &M, pw_t ex, const 
     return 0xFFFFFFFFu;
 }
 
-__global__ void finalize_kernel(const PrimeDesc *primes, const ProfDesc *profs, const ProfState *state,
-                                const u32 *dense_prefix, u32 nprof, u32 verify, OutRecord *out) {
-    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= nprof) return;
+// the record of profile g: M and witness from its best key, L (dense: from the
+// scan; sparse: by direct powers), optional certification, K.  The key and
+// status words are read through volatile loads: in the serving runtime the
+// last CTA leaving a profile finalises it while other CTAs' atomics on them
+// have just completed.
+__device__ inline void finalize_one(const PrimeDesc *primes, const ProfDesc *profs, const ProfState *state,
+                                    const u32 *dense_prefix, u32 g, u32 verify, OutRecord *out) {
     const ProfDesc D = profs[g];
     const PrimeDesc P = primes[D.prime];
-    const ProfState S = state[g];
+    const unsigned long long best = *(const volatile unsigned long long *)&state[g].best;
+    const u32 sstatus = *(const volatile u32 *)&state[g].status;
     const Mont M{P.p, P.ninv, P.one, P.r2};
     const pw_t p = P.p, ex = (p - 1u) / D.r;
     const u32 r = D.r;
-    u32 status = P.status | S.status;
-    const u32 Mlen = key_len(S.best), w = key_witness(S.best);
-    if (S.best == 0ull && !(D.qspec && P.route == 2u)) status |= ST_VERIFY;
+    u32 status = P.status | sstatus;
+    const u32 Mlen = key_len(best), w = key_witness(best);
+    if (best == 0ull && !(D.qspec && P.route == 2u)) status |= ST_VERIFY;
     if (P.route == 2u && D.qspec && Mlen < D.qspec) status |= ST_SPEC;
     u32 L;
     if (P.route == 1u) {
@@ -140,6 +144,12 @@ __global__ void finalize_kernel(const PrimeDesc *primes, const ProfDesc *profs, 
     const u64 b = ((((u64)p - 1u) / 2u) % r == 0u) ? 2ull * L + 2ull : (u64)L + 2ull;
     o.K = (u64)Mlen + 1ull > b ? (u64)Mlen + 1ull : b;
     out[D.out_slot] = o;
+}
+
+__global__ void finalize_kernel(const PrimeDesc *primes, const ProfDesc *profs, const ProfState *state,
+                                const u32 *dense_prefix, u32 nprof, u32 verify, OutRecord *out) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < nprof) finalize_one(primes, profs, state, dense_prefix, g, verify, out);
 }
 
 }  // namespace CZ_NS

@@ -1,51 +1,40 @@
 // runtime.cuh -- host runtime above the census entry points: the census of a
-// prime interval (device sieve + census) and the serving loop (request queue,
-// continuous batching over slots, admission by device memory, per-request
-// results held until polled).  Included once, at the end of census.cu; it
-// uses only the C ABI of include/rabung_census.h and the plane-pool estimate.
+// prime interval (device sieve + census) and the serving runtime.  Included
+// once, at the end of census.cu.
 //
-// Serving design:
-//  * one worker thread per slot, each owning one handle (one CUDA stream), so
-//    batches of different slots overlap on the device;
-//  * a free slot admits waiting requests in arrival order while their
-//    estimated colour-plane pools fit min(slot budget, free HBM - reserve)
-//    (always at least one request) and their flags match the first one's;
-//  * the batch's intervals are sieved in one device call, the primes of all
-//    its requests censused in one call (one persistent filter launch), and
-//    the records split back per request in submission order;
-//  * a refused merged call is re-run request by request, so only the request
-//    that caused the refusal is refused.
+// Serving design (the reference has no serving path; its supervisor feeds
+// fixed blocks to worker processes, src/census/worker32.cu:10-45):
+//  * one scheduler thread owns the GPU work; requests wait in arrival order;
+//  * every admitted request stays resident until its records are final: its
+//    sparse primes' descriptors, per-profile state, colour planes, records and
+//    A4 live in device arrays sized at open (ranges handed out first-fit), so
+//    admission is by free plane memory and free descriptor space;
+//  * the anchor filter runs as one persistent kernel over the unfinished
+//    profiles of every admitted request.  When requests arrive, the scheduler
+//    sets the kernel's yield flag: its CTAs finish the work item in hand,
+//    leave their profiles (the claim state stays in device memory) and exit;
+//    the new requests are sieved, planned and tabled on the whole GPU, and the
+//    kernel is relaunched over the old and new unfinished profiles together,
+//    so an arrival waits one work item (tens of microseconds), not a batch;
+//  * the last CTA to leave a finished profile certifies and writes its record
+//    and counts the request down; a request's last profile raises its done
+//    flag in mapped host memory, and the scheduler copies its records out
+//    while the kernel keeps running;
+//  * primes routed to the dense scan (small p), primes whose sparse record
+//    needs the dense re-run, and refusals are handled by a second handle in
+//    the window between launches; speculative thresholds are off here (a miss
+//    would need a re-run), which changes no record.
 #pragma once
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <map>
 #include <thread>
 #include <unordered_map>
 
 namespace {
 
-struct CzRequest {
-    uint64_t id = 0;
-    uint32_t lo = 0, count = 0, flags = 0;
-    bool given = false;                 // primes supplied by the caller
-    int rc = -1;                        // -1 while pending
-    std::string err;
-    std::vector<uint32_t> primes;
-    std::vector<cz_profile> recs;
-    std::vector<uint32_t> a4;
-    uint64_t est = 0;                   // colour-plane pool estimate, bytes
-};
-
-// plane-pool estimate of a request for `count` primes from lo: the pool of one
-// prime near the top of the interval (prime number theorem with slack) times
-// the count
-uint64_t interval_estimate(const cz_config &c, uint32_t lo, uint32_t count, uint32_t flags) {
-    const double span = (double)count * std::max(1.0, std::log((double)lo + 2.0)) * 1.3;
-    const double top = std::min(4294967291.0, (double)lo + span);
-    return plane_bytes(c, (uint32_t)top, flags) * (uint64_t)count;
-}
-
-// census of `primes` into r (records and A4), on handle h
+// census of `primes` into recs (and A4), on handle h
 int census_into(cz_handle *h, const std::vector<uint32_t> &primes, uint32_t flags, std::vector<cz_profile> &recs,
                 std::vector<uint32_t> &a4) {
     const uint32_t n = (uint32_t)primes.size();
@@ -56,100 +45,446 @@ int census_into(cz_handle *h, const std::vector<uint32_t> &primes, uint32_t flag
                      (flags & CZ_A4) ? a4.data() : nullptr, nullptr);
 }
 
+// first-fit ranges of [0, cap)
+struct Ranges {
+    std::map<u64, u64> free_;          // start -> length
+    void init(u64 cap) { free_.clear(); if (cap) free_[0] = cap; }
+    bool alloc(u64 n, u64 &off) {
+        if (n == 0) { off = 0; return true; }
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < n) continue;
+            off = it->first;
+            const u64 rest = it->second - n, start = it->first + n;
+            free_.erase(it);
+            if (rest) free_[start] = rest;
+            return true;
+        }
+        return false;
+    }
+    void release(u64 off, u64 n) {
+        if (n == 0) return;
+        auto it = free_.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) { it->second += nx->second; free_.erase(nx); }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) { pv->second += it->second; free_.erase(it); }
+        }
+    }
+};
+
+struct CzRequest {
+    uint64_t id = 0;
+    uint32_t lo = 0, count = 0, flags = 0;
+    bool given = false;                 // primes supplied by the caller
+    int rc = -1;                        // -1 while pending
+    std::string err;
+    std::vector<uint32_t> primes;
+    std::vector<cz_profile> recs;
+    std::vector<uint32_t> a4;
+    // resident part (sparse primes)
+    uint32_t slot = 0xFFFFFFFFu;        // request slot: pending counter and done flag
+    u64 pbase = 0, np = 0, gbase = 0, ng = 0, wbase = 0, nw = 0;
+    std::vector<uint32_t> list;         // global profile indices, launch order
+    std::vector<uint8_t> sparse;        // per prime: 1 resident, 0 censused on the second handle
+    std::vector<cz_profile> drecs;      // records of the other primes, in prime order
+    std::vector<uint32_t> da4;
+};
+
+constexpr u32 SRV_CAP_PRIMES = 1u << 20;       // resident primes
+constexpr u32 SRV_CAP_PROFILES = 1u << 22;     // resident profiles
+constexpr u32 SRV_CAP_SLOTS = 1u << 16;        // requests in flight
+
 }  // namespace
 
 struct cz_server {
     cz_config cfg{};
-    std::vector<cz_handle *> slots;
-    std::vector<std::thread> threads;
+    cz_handle *h = nullptr;             // stream, static tables; its buffers are unused
+    cz_handle *aux = nullptr;           // sieve, plans, dense primes, dense re-runs
+    PrimeDesc *d_primes = nullptr;
+    ProfDesc *d_profs = nullptr;
+    ProfState *d_state = nullptr;
+    OutRecord *d_out = nullptr;
+    u32 *d_a4 = nullptr, *d_list = nullptr, *d_sidx = nullptr, *d_next = nullptr, *d_pending = nullptr;
+    u32 *d_yield = nullptr, *d_a4err = nullptr, *d_planes = nullptr;
+    u32 *h_done = nullptr, *d_done = nullptr;   // mapped host flags, per request slot
+    u32 *h_flag = nullptr;                      // pinned: [0] = 1 (yield), [1] = a4 error word
+    u64 plane_words = 0;
+    Ranges rp, rg, rw, rs;
+    cudaStream_t cst = nullptr;                 // copies while the filter runs
+    cudaEvent_t ev_kernel = nullptr;
+    bool running = false, yielding = false;
+    std::vector<CzRequest *> inflight, deferred, repair;
+    std::thread sched;
     std::mutex m;
     std::condition_variable cv_work, cv_done;
     std::deque<CzRequest *> waiting;
     std::unordered_map<uint64_t, CzRequest *> reqs;
     std::deque<uint64_t> announced;     // completed, not yet returned by cz_next_done
-    uint64_t next_id = 1, budget = 0, reserve = 2ull << 30;
-    uint32_t max_batch = 4096;
+    uint64_t next_id = 1, launches = 0, completed = 0;
     bool stop = false;
-    uint64_t batches = 0, completed = 0;
     std::string err;
 };
 
 namespace {
 
-void run_batch(cz_server *s, cz_handle *h, std::vector<CzRequest *> &b) {
-    // device sieve of every interval of the batch, one call
-    std::vector<uint32_t> lo, cnt;
-    std::vector<CzRequest *> sv;
-    for (CzRequest *r : b)
-        if (!r->given) { lo.push_back(r->lo); cnt.push_back(r->count); sv.push_back(r); }
-    if (!sv.empty()) {
-        uint64_t tot = 0;
-        for (uint32_t c : cnt) tot += c;
-        std::vector<uint32_t> out(std::max<uint64_t>(1, tot)), found(sv.size());
-        const int rc = cz_sieve(h, lo.data(), cnt.data(), (uint32_t)sv.size(), out.data(), found.data());
-        uint64_t off = 0;
-        for (size_t i = 0; i < sv.size(); ++i) {
-            if (rc) { sv[i]->rc = rc; sv[i]->err = cz_last_error(h); continue; }
-            sv[i]->primes.assign(out.begin() + off, out.begin() + off + found[i]);
-            off += cnt[i];
+void finish(cz_server *s, CzRequest *r, int rc, const std::string &err = "") {
+    r->rc = rc;
+    r->err = err;
+    if (rc) { r->recs.clear(); r->a4.clear(); }
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        s->announced.push_back(r->id);
+        ++s->completed;
+    }
+    s->cv_done.notify_all();
+}
+
+void release(cz_server *s, CzRequest *r) {
+    s->rp.release(r->pbase, r->np);
+    s->rg.release(r->gbase, r->ng);
+    s->rw.release(r->wbase, r->nw);
+    if (r->slot != 0xFFFFFFFFu) s->rs.release(r->slot, 1);
+    r->np = r->ng = r->nw = 0;
+    r->slot = 0xFFFFFFFFu;
+}
+
+// records of a request in prime order: resident primes from the device
+// arrays, the others from the second handle; primes needing the dense re-run
+// are collected in *redo
+int assemble(cz_server *s, CzRequest *r, std::vector<uint32_t> *redo) {
+    std::vector<OutRecord> dev(r->ng);
+    std::vector<u32> dva4(r->np);
+    u32 a4err = 0;
+    if (r->np && (r->flags & CZ_A4) &&
+        cudaMemcpyAsync(&a4err, s->d_a4err + r->slot, 4, cudaMemcpyDeviceToHost, s->cst) != cudaSuccess)
+        return CZ_ECUDA;
+    if (r->ng && cudaMemcpyAsync(dev.data(), s->d_out + r->gbase, sizeof(OutRecord) * r->ng, cudaMemcpyDeviceToHost,
+                                 s->cst) != cudaSuccess)
+        return CZ_ECUDA;
+    if ((r->flags & CZ_A4) && r->np &&
+        cudaMemcpyAsync(dva4.data(), s->d_a4 + r->pbase, 4ull * r->np, cudaMemcpyDeviceToHost, s->cst) != cudaSuccess)
+        return CZ_ECUDA;
+    if (cudaStreamSynchronize(s->cst) != cudaSuccess) return CZ_ECUDA;
+    if (a4err) { r->err = "refused: A4 point count not certified"; return CZ_EREFUSED; }
+    r->recs.clear();
+    r->a4.assign((r->flags & CZ_A4) ? r->primes.size() : 0u, 0u);
+    size_t gi = 0, di = 0, pi = 0, dpi = 0;
+    for (size_t i = 0; i < r->primes.size(); ++i) {
+        const u32 k = r->primes[i] > 2u ? popc(mask_of(r->primes[i])) : 0u;
+        if (r->sparse[i]) {
+            for (u32 j = 0; j < k; ++j, ++gi) {
+                const OutRecord &o = dev[gi];
+                if (o.status) {
+                    if (!(o.status & (ST_ROOT | ST_LABEL | ST_VERIFY))) {
+                        if (redo && (redo->empty() || redo->back() != (u32)i)) redo->push_back((u32)i);
+                    } else {
+                        char buf[160];
+                        snprintf(buf, sizeof buf, "refused: p=%u r=%u status=0x%x", o.p, o.r, o.status);
+                        r->err = buf;
+                        return CZ_EREFUSED;
+                    }
+                }
+                r->recs.push_back(cz_profile{o.p, o.r, o.M, o.L, o.witness, o.status, o.K});
+            }
+            if (r->flags & CZ_A4) r->a4[i] = dva4[pi];
+            ++pi;
+        } else {
+            for (u32 j = 0; j < k; ++j) r->recs.push_back(r->drecs[di++]);
+            if (r->flags & CZ_A4) r->a4[i] = r->da4[dpi];
+            ++dpi;
         }
     }
-    std::vector<CzRequest *> live;
-    std::vector<uint32_t> flat;
-    for (CzRequest *r : b)
-        if (r->rc < 0) { live.push_back(r); flat.insert(flat.end(), r->primes.begin(), r->primes.end()); }
-    if (live.empty()) return;
-    const uint32_t flags = live.front()->flags;
+    return CZ_OK;
+}
+
+// dense re-run of the primes of r listed in redo (indices into r->primes),
+// patching their records in place (the window between launches only)
+int repair(cz_server *s, CzRequest *r, const std::vector<u32> &redo) {
+    std::vector<u32> ps, first;
+    size_t off = 0;
+    std::vector<size_t> start(r->primes.size());
+    for (size_t i = 0; i < r->primes.size(); ++i) {
+        start[i] = off;
+        off += r->primes[i] > 2u ? popc(mask_of(r->primes[i])) : 0u;
+    }
+    for (u32 i : redo) ps.push_back(r->primes[i]);
     std::vector<cz_profile> recs;
     std::vector<uint32_t> a4;
-    const int rc = census_into(h, flat, flags, recs, a4);
-    if (rc == CZ_OK) {
-        size_t pp = 0, rp = 0;
-        for (CzRequest *r : live) {
-            const uint32_t np = cz_count_profiles(r->primes.data(), (uint32_t)r->primes.size());
-            r->recs.assign(recs.begin() + rp, recs.begin() + rp + np);
-            if (flags & CZ_A4) r->a4.assign(a4.begin() + pp, a4.begin() + pp + r->primes.size());
-            rp += np;
-            pp += r->primes.size();
-            r->rc = CZ_OK;
-        }
-        return;
+    const int rc = census_into(s->aux, ps, (r->flags & ~(CZ_AUTO | CZ_A4)) | CZ_DENSE, recs, a4);
+    if (rc) { r->err = cz_last_error(s->aux); return rc; }
+    size_t t = 0;
+    for (u32 i : redo) {
+        const u32 k = popc(mask_of(r->primes[i]));
+        for (u32 j = 0; j < k; ++j) r->recs[start[i] + j] = recs[t++];
     }
-    for (CzRequest *r : live) {            // attribute the refusal: each request alone
-        const int rr = live.size() == 1 ? rc : census_into(h, r->primes, flags, r->recs, r->a4);
-        r->rc = rr;
-        if (rr) { r->err = cz_last_error(h); r->recs.clear(); r->a4.clear(); }
+    return CZ_OK;
+}
+
+// requests whose done flag is up: records out (while the filter runs), then
+// complete, or queue for a dense re-run in the next window
+void poll_done(cz_server *s) {
+    for (size_t i = 0; i < s->inflight.size();) {
+        CzRequest *r = s->inflight[i];
+        if (!*(volatile u32 *)&s->h_done[r->slot]) { ++i; continue; }
+        s->inflight.erase(s->inflight.begin() + i);
+        std::vector<u32> redo;
+        const int rc = assemble(s, r, &redo);
+        s->deferred.push_back(r);                       // its ranges are freed after this launch
+        if (rc) { finish(s, r, rc, r->err.empty() ? std::string("record copy failed") : r->err); continue; }
+        if (!redo.empty()) { s->repair.push_back(r); continue; }
+        finish(s, r, CZ_OK);
     }
 }
 
-void slot_loop(cz_server *s, size_t k) {
-    cz_handle *h = s->slots[k];
-    for (;;) {
-        uint64_t fr = 0, tot = 0;
-        cz_mem_info(h, &fr, &tot);
-        std::vector<CzRequest *> batch;
-        {
-            std::unique_lock<std::mutex> lk(s->m);
-            s->cv_work.wait(lk, [s] { return s->stop || !s->waiting.empty(); });
-            if (s->stop) return;
-            const uint64_t cap = std::min<uint64_t>(s->budget, fr > s->reserve ? fr - s->reserve : 0);
-            const uint32_t flags = s->waiting.front()->flags;
-            uint64_t used = 0;
-            for (auto it = s->waiting.begin(); it != s->waiting.end() && batch.size() < s->max_batch;) {
-                CzRequest *r = *it;
-                if (r->flags != flags || (!batch.empty() && used + r->est > cap)) { ++it; continue; }
-                batch.push_back(r);
-                used += r->est;
-                it = s->waiting.erase(it);
-            }
-            ++s->batches;
+// requests out of flight whose records carry a fallback status: re-run those
+// primes on the dense scan (the window between launches only)
+void run_repairs(cz_server *s) {
+    for (CzRequest *r : s->repair) {
+        std::vector<u32> redo;
+        size_t off = 0;
+        for (size_t i = 0; i < r->primes.size(); ++i) {
+            const u32 k = r->primes[i] > 2u ? popc(mask_of(r->primes[i])) : 0u;
+            for (u32 j = 0; j < k; ++j)
+                if (r->recs[off + j].status) { redo.push_back((u32)i); break; }
+            off += k;
         }
-        run_batch(s, h, batch);
+        const int rc = repair(s, r, redo);
+        finish(s, r, rc, rc ? r->err : std::string());
+    }
+    s->repair.clear();
+}
+
+// admit waiting requests while they fit; sieve, plan, upload, set up, table
+// and A4 on the whole GPU (no filter kernel runs now)
+void admit(cz_server *s) {
+    std::vector<CzRequest *> batch;
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        while (!s->waiting.empty() && batch.size() < 4096) { batch.push_back(s->waiting.front()); s->waiting.pop_front(); }
+    }
+    if (batch.empty()) return;
+    cudaStream_t st = s->h->st;
+    std::vector<u32> sidx;                              // global indices of new resident primes
+    std::vector<CzRequest *> back;                      // did not fit now
+    u32 table_smem = 0;
+    std::vector<u32> pend_slot, pend_val;
+    std::vector<CzRequest *> admitted;                  // requests given resident space in this window
+    // a request that does not fit the empty server is refused; one that does
+    // not fit now waits, with everything behind it, for space to free up
+    auto no_room = [&](CzRequest *r) {
+        if (s->inflight.empty() && s->deferred.empty() && admitted.empty())
+            finish(s, r, CZ_ELIMIT, "request exceeds the server's prime, profile or plane capacity");
+        else
+            back.push_back(r);
+    };
+    for (size_t bi = 0; bi < batch.size(); ++bi) {
+        CzRequest *r = batch[bi];
+        if (!back.empty()) { back.push_back(r); continue; }
+        if (!r->given) {
+            std::vector<uint32_t> got(r->count);
+            uint32_t found = 0;
+            const int rc = cz_sieve(s->aux, &r->lo, &r->count, 1, got.data(), &found);
+            if (rc) { finish(s, r, rc, cz_last_error(s->aux)); continue; }
+            got.resize(found);
+            r->primes.swap(got);
+        }
+        const u32 n = (u32)r->primes.size();
+        if (n == 0) { r->recs.clear(); r->a4.clear(); finish(s, r, CZ_OK); continue; }
+        u32 mode = r->flags & CZ_AUTO;
+        if (!mode) mode = CZ_AUTO;
+        int rc = plan(s->aux, r->primes.data(), n, mode | CZ_NOSPEC);
+        if (rc) { finish(s, r, rc, s->aux->err); continue; }
+        // the resident (sparse) part of the plan
+        std::vector<PrimeDesc> hp;
+        std::vector<ProfDesc> hg;
+        std::vector<u32> slist_local;                   // plan's filter order, as local profile indices
+        r->sparse.assign(n, 0u);
+        u64 words = 0;
+        for (u32 i = 0; i < n; ++i)
+            if (s->aux->hp[i].route == 2u) r->sparse[i] = 1u;
+        std::vector<u32> gmap(s->aux->nprof, 0xFFFFFFFFu);
+        for (u32 i = 0; i < n; ++i) {
+            if (!r->sparse[i]) continue;
+            const PrimeDesc &P = s->aux->hp[i];
+            for (u32 j = 0; j < P.nprof; ++j) {
+                const ProfDesc &D = s->aux->hprof[P.first_prof + j];
+                const u64 pw = ((u64)D.npp * (P.nwords + P.nwords2) + 7ull) & ~7ull;
+                words = std::max<u64>(words, D.plane_off + pw);
+            }
+        }
+        u64 np = 0;
+        for (u32 i = 0; i < n; ++i) np += r->sparse[i];
+        u64 ng = 0;
+        for (u32 i = 0; i < n; ++i) if (r->sparse[i]) ng += s->aux->hp[i].nprof;
+        if (np) {
+            u64 pb = 0, gb = 0, wb = 0, sl = 0;
+            if (words > s->plane_words) {
+                finish(s, r, CZ_ELIMIT, "request's colour planes exceed the server's plane budget");
+                continue;
+            }
+            if (!s->rp.alloc(np, pb)) { no_room(r); continue; }
+            if (!s->rg.alloc(ng, gb)) { s->rp.release(pb, np); no_room(r); continue; }
+            if (!s->rw.alloc(words, wb)) { s->rp.release(pb, np); s->rg.release(gb, ng); no_room(r); continue; }
+            if (!s->rs.alloc(1, sl)) {
+                s->rp.release(pb, np); s->rg.release(gb, ng); s->rw.release(wb, words);
+                no_room(r);
+                continue;
+            }
+            r->pbase = pb; r->np = np; r->gbase = gb; r->ng = ng; r->wbase = wb; r->nw = words; r->slot = (u32)sl;
+            u32 k = 0, gcount = 0;
+            for (u32 i = 0; i < n; ++i) {
+                if (!r->sparse[i]) continue;
+                PrimeDesc P = s->aux->hp[i];
+                const u32 f0 = P.first_prof;
+                P.first_prof = (u32)(gb + gcount);
+                for (u32 j = 0; j < P.nprof; ++j) {
+                    ProfDesc D = s->aux->hprof[f0 + j];
+                    D.prime = (u32)(pb + k);
+                    D.out_slot = (u32)(gb + gcount + j);
+                    D.plane_off += wb;
+                    D.req = (u32)sl;
+                    gmap[f0 + j] = (u32)(gb + gcount + j);
+                    hg.push_back(D);
+                }
+                gcount += P.nprof;
+                hp.push_back(P);
+                sidx.push_back((u32)(pb + k));
+                ++k;
+            }
+            for (u32 g : s->aux->h_slist)
+                if (gmap[g] != 0xFFFFFFFFu) r->list.push_back(gmap[g]);
+            table_smem = std::max(table_smem, s->aux->table_smem);
+            cudaMemcpyAsync(s->d_primes + pb, hp.data(), sizeof(PrimeDesc) * np, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(s->d_profs + gb, hg.data(), sizeof(ProfDesc) * ng, cudaMemcpyHostToDevice, st);
+            setup_kernel<<<(u32)((np + 127) / 128), 128, 0, st>>>(s->d_primes + pb, s->d_profs, s->d_state, (u32)np);
+            cudaMemsetAsync(s->d_a4err + sl, 0, 4, st);    // this request's A4 error word
+            if (r->flags & CZ_A4)
+                a4_kernel<<<(u32)((np + A4_WARPS - 1) / A4_WARPS), A4_WARPS * 32, 0, st>>>(s->d_primes + pb, (u32)np,
+                                                                                     s->d_a4 + pb, s->d_a4err + sl);
+            s->h_done[sl] = 0u;
+            admitted.push_back(r);
+            pend_slot.push_back((u32)sl);
+            pend_val.push_back((u32)ng);
+        }
+        // the other primes on the second handle (dense scan), in prime order
+        std::vector<uint32_t> other;
+        for (u32 i = 0; i < n; ++i) if (!r->sparse[i]) other.push_back(r->primes[i]);
+        rc = census_into(s->aux, other, (r->flags & ~CZ_AUTO) | CZ_DENSE, r->drecs, r->da4);
+        if (rc) { release(s, r); finish(s, r, rc, cz_last_error(s->aux)); continue; }
+        if (!np) {
+            const int arc = assemble(s, r, nullptr);
+            finish(s, r, arc, arc ? r->err : std::string());
+            continue;
+        }
+        s->inflight.push_back(r);
+    }
+    if (!sidx.empty()) {
+        for (size_t i = 0; i < pend_slot.size(); ++i)
+            cudaMemcpyAsync(s->d_pending + pend_slot[i], &pend_val[i], 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(s->d_sidx, sidx.data(), 4ull * sidx.size(), cudaMemcpyHostToDevice, st);
+        TableArgs ta;
+        ta.primes = s->d_primes;
+        ta.profs = s->d_profs;
+        ta.state = s->d_state;
+        ta.planes = s->d_planes;
+        ta.sparse_primes = s->d_sidx;
+        ta.nsparse = (u32)sidx.size();
+        ta.small_primes = s->h->d_small;
+        ta.n_small = s->h->n_small;
+        ta.chain = s->h->d_chain;
+        ta.chain_limit = CHAIN_LIMIT;
+        table_kernel<<<std::min<u32>(ta.nsparse, (u32)s->h->sms), TABLE_THREADS, table_smem, st>>>(ta);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            for (CzRequest *r : s->inflight) { release(s, r); finish(s, r, CZ_ECUDA, "set-up kernels failed"); }
+            s->inflight.clear();
+        }
+    }
+    if (!back.empty()) {
+        std::lock_guard<std::mutex> lk(s->m);
+        for (auto it = back.rbegin(); it != back.rend(); ++it) s->waiting.push_front(*it);
+    }
+}
+
+// launch the filter over the unfinished profiles of every request in flight
+void launch(cz_server *s) {
+    std::vector<u32> list;
+    for (CzRequest *r : s->inflight) list.insert(list.end(), r->list.begin(), r->list.end());
+    if (list.empty()) return;
+    cudaStream_t st = s->h->st;
+    cudaMemcpyAsync(s->d_list, list.data(), 4ull * list.size(), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(s->d_next, 0, 4, st);
+    cudaMemsetAsync(s->d_yield, 0, 4, st);
+    SparseArgs sa{};
+    sa.primes = s->d_primes;
+    sa.profs = s->d_profs;
+    sa.state = s->d_state;
+    sa.planes = s->d_planes;
+    sa.prof_list = s->d_list;
+    sa.nlist = (u32)list.size();
+    sa.next = s->d_next;
+    u32 grid = s->cfg.sparse_blocks ? s->cfg.sparse_blocks : (u32)CZ_SPARSE_MINB * (u32)s->h->sms;
+    sa.group = std::max(std::max(1u, s->cfg.cta_per_profile), std::min(64u, grid / std::max(1u, sa.nlist)));
+    sa.tune.screen = s->cfg.screen;
+    sa.epoch_rows = s->cfg.epoch_rows;
+    sa.yield = s->d_yield;
+    sa.out = s->d_out;
+    sa.verify = 1u;
+    sa.req_pending = s->d_pending;
+    sa.req_done = s->d_done;
+    grid = std::min(grid, sa.nlist * sa.group);
+    // the list copy above comes from pageable memory: it is staged before the
+    // call returns, so `list` may go; the kernel runs on while the scheduler polls
+    sparse_kernel<<<grid, SPARSE_WARPS * 32, TILE_WORDS * 4u, st>>>(sa);
+}
+
+void sched_loop(cz_server *s) {
+    cudaSetDevice(s->h->dev);
+    for (;;) {
+        poll_done(s);
+        bool have_waiting, stopping;
         {
             std::lock_guard<std::mutex> lk(s->m);
-            for (CzRequest *r : batch) { s->announced.push_back(r->id); ++s->completed; }
+            have_waiting = !s->waiting.empty();
+            stopping = s->stop;
         }
-        s->cv_done.notify_all();
+        if (s->running) {
+            if ((have_waiting || stopping || !s->repair.empty()) && !s->yielding) {
+                cudaMemcpyAsync(s->d_yield, &s->h_flag[0], 4, cudaMemcpyHostToDevice, s->cst);
+                s->yielding = true;
+            }
+            if (cudaEventQuery(s->ev_kernel) != cudaSuccess) {
+                std::unique_lock<std::mutex> lk(s->m);
+                s->cv_work.wait_for(lk, std::chrono::microseconds(100));
+                continue;
+            }
+            cudaStreamSynchronize(s->cst);
+            s->running = false;
+            poll_done(s);
+            if (!s->yielding) {                        // a launch that ran to its end finished every profile
+                for (CzRequest *r : s->inflight) {
+                    s->deferred.push_back(r);
+                    finish(s, r, CZ_EREFUSED, "refused: a profile did not finish");
+                }
+                s->inflight.clear();
+            }
+            s->yielding = false;
+        }
+        for (CzRequest *r : s->deferred) release(s, r);
+        s->deferred.clear();
+        if (stopping) return;
+        run_repairs(s);
+        admit(s);
+        if (!s->inflight.empty()) {
+            launch(s);
+            cudaEventRecord(s->ev_kernel, s->h->st);
+            s->running = true;
+            std::lock_guard<std::mutex> lk(s->m);
+            ++s->launches;
+            continue;
+        }
+        std::unique_lock<std::mutex> lk(s->m);
+        s->cv_work.wait(lk, [s] { return s->stop || !s->waiting.empty(); });
     }
 }
 
@@ -158,6 +493,21 @@ template <class Pred>
 bool wait_for(std::condition_variable &cv, std::unique_lock<std::mutex> &lk, int32_t timeout_ms, Pred pred) {
     if (timeout_ms < 0) { cv.wait(lk, pred); return true; }
     return cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred);
+}
+
+void server_free(cz_server *s) {
+    cudaSetDevice(s->h ? s->h->dev : 0);
+    void *dev[] = {s->d_primes, s->d_profs, s->d_state, s->d_out, s->d_a4, s->d_list, s->d_sidx, s->d_next,
+                   s->d_pending, s->d_yield, s->d_a4err, s->d_planes};
+    for (void *p : dev) if (p) cudaFree(p);
+    if (s->h_done) cudaFreeHost(s->h_done);
+    if (s->h_flag) cudaFreeHost(s->h_flag);
+    if (s->ev_kernel) cudaEventDestroy(s->ev_kernel);
+    if (s->cst) cudaStreamDestroy(s->cst);
+    if (s->aux) cz_close(s->aux);
+    if (s->h) cz_close(s->h);
+    for (auto &kv : s->reqs) delete kv.second;
+    delete s;
 }
 
 }  // namespace
@@ -209,18 +559,46 @@ int cz_server_open(const cz_config *cfg, uint32_t slots, uint64_t slot_budget_by
     *out = nullptr;
     cz_server *s = new cz_server();
     if (cfg) s->cfg = *cfg; else cz_default_config(&s->cfg);
-    s->budget = slot_budget_bytes ? slot_budget_bytes : ((uint64_t)s->cfg.plane_budget_mb << 20);
-    for (uint32_t k = 0; k < slots; ++k) {
-        cz_handle *h = nullptr;
-        const int rc = cz_open(&s->cfg, &h);
-        if (rc) {
-            for (cz_handle *x : s->slots) cz_close(x);
-            delete s;
-            return rc;
-        }
-        s->slots.push_back(h);
-    }
-    for (size_t k = 0; k < s->slots.size(); ++k) s->threads.emplace_back(slot_loop, s, k);
+    s->cfg.speculate = 0;                       // a speculative miss would need a re-run
+    int rc = cz_open(&s->cfg, &s->h);
+    if (!rc) rc = cz_open(&s->cfg, &s->aux);
+    if (rc) { server_free(s); return rc; }
+    cudaSetDevice(s->h->dev);
+    const u64 per = slot_budget_bytes ? slot_budget_bytes : ((u64)s->cfg.plane_budget_mb << 20);
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    const u64 fixed = (u64)SRV_CAP_PRIMES * (sizeof(PrimeDesc) + 8) +
+                      (u64)SRV_CAP_PROFILES * (sizeof(ProfDesc) + sizeof(ProfState) + sizeof(OutRecord) + 4) +
+                      (u64)SRV_CAP_SLOTS * 4 + (4ull << 30);
+    u64 planes = (u64)slots * per;
+    if (fr > fixed && planes > (u64)fr - fixed) planes = (u64)fr - fixed;
+    s->plane_words = planes / 4ull & ~7ull;
+    bool ok = cudaMalloc(&s->d_primes, sizeof(PrimeDesc) * SRV_CAP_PRIMES) == cudaSuccess &&
+              cudaMalloc(&s->d_profs, sizeof(ProfDesc) * SRV_CAP_PROFILES) == cudaSuccess &&
+              cudaMalloc(&s->d_state, sizeof(ProfState) * SRV_CAP_PROFILES) == cudaSuccess &&
+              cudaMalloc(&s->d_out, sizeof(OutRecord) * SRV_CAP_PROFILES) == cudaSuccess &&
+              cudaMalloc(&s->d_a4, 4ull * SRV_CAP_PRIMES) == cudaSuccess &&
+              cudaMalloc(&s->d_list, 4ull * SRV_CAP_PROFILES) == cudaSuccess &&
+              cudaMalloc(&s->d_sidx, 4ull * SRV_CAP_PRIMES) == cudaSuccess &&
+              cudaMalloc(&s->d_next, 64) == cudaSuccess && cudaMalloc(&s->d_yield, 64) == cudaSuccess &&
+              cudaMalloc(&s->d_a4err, 4ull * SRV_CAP_SLOTS) == cudaSuccess &&
+              cudaMalloc(&s->d_pending, 4ull * SRV_CAP_SLOTS) == cudaSuccess &&
+              cudaMalloc(&s->d_planes, 4ull * std::max<u64>(8, s->plane_words)) == cudaSuccess &&
+              cudaHostAlloc(&s->h_done, 4ull * SRV_CAP_SLOTS, cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&s->d_done, s->h_done, 0) == cudaSuccess &&
+              cudaHostAlloc(&s->h_flag, 64, cudaHostAllocDefault) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->cst, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&s->ev_kernel, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) { server_free(s); return CZ_ECUDA; }
+    s->h_flag[0] = 1u;
+    std::memset(s->h_done, 0, 4ull * SRV_CAP_SLOTS);
+    cudaMemset(s->d_yield, 0, 64);
+    cudaMemset(s->d_a4err, 0, 4ull * SRV_CAP_SLOTS);
+    s->rp.init(SRV_CAP_PRIMES);
+    s->rg.init(SRV_CAP_PROFILES);
+    s->rw.init(s->plane_words);
+    s->rs.init(SRV_CAP_SLOTS);
+    s->sched = std::thread(sched_loop, s);
     *out = s;
     return CZ_OK;
 }
@@ -233,10 +611,8 @@ void cz_server_close(cz_server *s) {
     }
     s->cv_work.notify_all();
     s->cv_done.notify_all();
-    for (std::thread &t : s->threads) t.join();
-    for (auto &kv : s->reqs) delete kv.second;
-    for (cz_handle *h : s->slots) cz_close(h);
-    delete s;
+    if (s->sched.joinable()) s->sched.join();
+    server_free(s);
 }
 
 int cz_submit(cz_server *s, uint32_t lo, uint32_t count, const uint32_t *primes, uint32_t flags,
@@ -249,9 +625,6 @@ int cz_submit(cz_server *s, uint32_t lo, uint32_t count, const uint32_t *primes,
     if (primes) {
         r->given = true;
         r->primes.assign(primes, primes + count);
-        for (uint32_t p : r->primes) r->est += plane_bytes(s->cfg, p, flags);
-    } else {
-        r->est = interval_estimate(s->cfg, lo, count, flags);
     }
     {
         std::lock_guard<std::mutex> lk(s->m);
@@ -308,7 +681,7 @@ int cz_poll(cz_server *s, uint64_t request_id, int32_t timeout_ms, uint32_t *pri
 int cz_server_info(cz_server *s, uint64_t *batches, uint64_t *completed, uint64_t *waiting) {
     if (!s) return CZ_EINVAL;
     std::lock_guard<std::mutex> lk(s->m);
-    if (batches) *batches = s->batches;
+    if (batches) *batches = s->launches;
     if (completed) *completed = s->completed;
     if (waiting) *waiting = s->waiting.size();
     return CZ_OK;

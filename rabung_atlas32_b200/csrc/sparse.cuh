@@ -51,6 +51,7 @@
 // global memory, and the screened candidates are completed 32 at a time.
 #pragma once
 #include "labels.cuh"
+#include "finalize.cuh"
 
 namespace CZ_NS {
 
@@ -97,6 +98,14 @@ struct SparseArgs {
     u32 group;                // CTAs that share one profile (its rows)
     Tuning tune;
     u32 epoch_rows;           // rows d per threshold epoch
+    // serving runtime only (out == nullptr otherwise): profiles span launches;
+    // the last CTA to leave a profile whose items are all done writes its
+    // record and counts its request down
+    const volatile u32 *yield;    // mapped host flag: set -> stop claiming, leave, return
+    OutRecord *out;               // records, by ProfDesc.out_slot
+    u32 verify;                   // certify each record (CZ_VERIFY)
+    u32 *req_pending;             // per request slot: sparse profiles not yet final
+    volatile u32 *req_done;       // mapped host memory, per request slot: 1 when all are final
 };
 
 struct Cand { u32 b, d; };
@@ -593,14 +602,43 @@ __device__ inline bool claim_item(const ProfCtx &c, ProfState *st, u32 &item, u3
     return false;
 }
 
+// hand out no further item of the profile (after an error: its record is
+// refused, and the serving runtime must still see the profile finish)
+__device__ inline void exhaust_claims(const ProfCtx &c, ProfState *st) {
+    unsigned long long old = *(volatile unsigned long long *)&st->claim;
+    for (int guard = 0; guard < 1 << 20 && (u32)old < c.nitems; ++guard) {
+        const unsigned long long prev = atomicCAS(&st->claim, old, (old & ~0xFFFFFFFFull) | c.nitems);
+        if (prev == old) break;
+        old = prev;
+    }
+}
+
+// serving: a CTA leaves profile g; the last one to leave a profile whose items
+// are all handed out writes its record (once) and counts its request down
+__device__ __noinline__ void leave_profile(const SparseArgs &a, const ProfCtx &c, u32 g) {
+    ProfState *st = a.state + g;
+    __threadfence();
+    const u32 left = atomicSub(&st->active, 1u) - 1u;
+    const u32 claimed = (u32)*(volatile unsigned long long *)&st->claim;
+    if (left != 0u || claimed < c.nitems || atomicCAS(&st->done, 0u, 1u) != 0u) return;
+    finalize_one(a.primes, a.profs, a.state, nullptr, g, a.verify, a.out);
+    __threadfence();
+    const u32 req = a.profs[g].req;
+    if (atomicSub(&a.req_pending[req], 1u) == 1u) {
+        __threadfence_system();
+        a.req_done[req] = 1u;
+    }
+}
+
 // thread 0: claim the profile's next work item, describe it in *out and start
 // the bulk copy of its tile into shared memory; false when the profile has no
 // item left (or on an error, reported in *err: 2 threshold below 3, 4 tile)
 __device__ __noinline__ bool next_item(const ProfCtx &c, ProfState *st, u32 erows, u32 tile, u32 mbar, Item *out,
-                                       u32 *err) {
+                                       u32 *err, const volatile u32 *yield) {
     u32 item = 0, qe = 0;
+    if (yield && *yield) { *err |= 8u; return false; }
     if (!claim_item(c, st, item, qe)) return false;
-    if (qe < 3u) { *err |= 2u; return false; }
+    if (qe < 3u) { *err |= 2u; exhaust_claims(c, st); return false; }
     Item it;
     const u32 ipe = c.nt[0] + c.nt[1], e = item / ipe, j = item - e * ipe;
     it.view = j < c.nt[0] ? 0u : 1u;
@@ -625,7 +663,7 @@ __device__ __noinline__ bool next_item(const ProfCtx &c, ProfState *st, u32 erow
     u32 w1 = w1r < (u64)nwv ? (u32)w1r : nwv;
     if (w1 < w0 + 4u) w1 = min(nwv, w0 + 4u);
     const u32 bytes = (w1 - w0) * c.npp * 4u;
-    if (bytes > TILE_WORDS * 4u || w1 <= w0) { *err |= 4u; return false; }
+    if (bytes > TILE_WORDS * 4u || w1 <= w0) { *err |= 4u; exhaust_claims(c, st); return false; }
     it.S = tile;
     it.ubase = 32u * w0;
     *out = it;
@@ -674,9 +712,13 @@ sparse_kernel(SparseArgs a) {
     for (;;) {
         if (threadIdx.x == 0) {
             // a.group consecutive CTA slots share one profile
-            s_item = atomicAdd(a.next, 1u) / a.group;
+            s_item = (a.yield && *a.yield) ? a.nlist : atomicAdd(a.next, 1u) / a.group;
             s_err = 0u;
-            if (s_item < a.nlist) load_profile(a, a.prof_list[s_item], &s_ctx, &s_err);
+            if (s_item < a.nlist) {
+                load_profile(a, a.prof_list[s_item], &s_ctx, &s_err);
+                if (a.out) atomicAdd(&a.state[a.prof_list[s_item]].active, 1u);
+                if (s_err & 4u) exhaust_claims(s_ctx, a.state + a.prof_list[s_item]);
+            }
         }
         __syncthreads();
         const u32 pitem = s_item;
@@ -690,7 +732,7 @@ sparse_kernel(SparseArgs a) {
             if (threadIdx.x == 0) {
                 u32 err = 0;
                 s_has = next_item(c, st, a.epoch_rows ? a.epoch_rows : EPOCH_ROWS_DEFAULT, smem_addr(s_tile),
-                                  smem_addr(&s_mbar), &s_it, &err) ? 1u : 0u;
+                                  smem_addr(&s_mbar), &s_it, &err, a.yield) ? 1u : 0u;
                 s_err |= err;
                 s_row = 0u;
             }
@@ -727,8 +769,12 @@ sparse_kernel(SparseArgs a) {
             atomicAdd(&st->tests, (unsigned long long)tests);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && s_err)
-            atomicOr(&st->status, (s_err & 2u) ? ST_SEED : ((s_err & 4u) ? ST_COVER : ST_QUEUE));
+        const u32 errs = s_err & 7u, yielded = s_err & 8u;
+        if (threadIdx.x == 0) {
+            if (errs) atomicOr(&st->status, (errs & 2u) ? ST_SEED : ((errs & 4u) ? ST_COVER : ST_QUEUE));
+            if (a.out) leave_profile(a, c, a.prof_list[pitem]);
+        }
+        if (yielded) return;
     }
 }
 

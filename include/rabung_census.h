@@ -176,18 +176,26 @@ int cz_census_interval(cz_handle *h, uint64_t lo, uint64_t hi, uint32_t flags, u
                        uint32_t *n_profiles, uint32_t *a4_out, cz_stats *stats);
 
 /* ---- serving ---------------------------------------------------------------
- * A server owns `slots` handles (one CUDA stream each) and one worker thread
- * per slot.  Requests wait in arrival order; whenever a slot is free it admits
- * every waiting request (same flags) whose colour-plane pool still fits the
- * slot budget and the GPU's free memory, sieves the batch's intervals on the
- * device, censuses the batch in one merged call and holds each request's
- * records until they are polled.  A merged call that is refused is re-run
- * request by request, so a refusal reaches only the request that caused it.
- * Submit and poll may be called from any host thread.  The reference has no
- * serving path; the records equal cz_census's for the same primes. */
+ * A server keeps every admitted request resident on the GPU until its records
+ * are final: the descriptors, per-profile state, colour planes, records and A4
+ * of its primes live in device arrays sized when the server opens (colour
+ * planes: slots x slot_budget_bytes, capped by free device memory), so a
+ * request is admitted as soon as its planes and descriptors fit.  The anchor
+ * filter runs as one persistent kernel over the unfinished profiles of all
+ * admitted requests; when requests arrive it yields between work items and is
+ * relaunched over the old and new profiles together, so an arrival joins the
+ * work in flight instead of waiting for a batch to end.  The last CTA to
+ * finish a profile certifies and writes its record; a request's records are
+ * copied out as soon as its last profile is final.  Primes below the sparse
+ * route (small p) and dense re-runs use a second handle between launches;
+ * speculative thresholds are off (records are unchanged by them).  A refusal
+ * reaches only the request that caused it; a request whose colour planes
+ * exceed the server's whole plane budget is refused.  Submit and poll may be
+ * called from any host thread.  The reference has no serving path; the
+ * records equal cz_census's for the same primes. */
 typedef struct cz_server cz_server;
 int cz_server_open(const cz_config *cfg, uint32_t slots, uint64_t slot_budget_bytes, cz_server **out);
-void cz_server_close(cz_server *s);             /* finishes running batches; drops unpolled work */
+void cz_server_close(cz_server *s);             /* stops the filter at its next work item; drops unpolled work */
 /* a request for the `count` consecutive primes from lo (device sieve), or,
  * when primes != NULL, for those `count` primes; flags as for cz_census */
 int cz_submit(cz_server *s, uint32_t lo, uint32_t count, const uint32_t *primes, uint32_t flags,
@@ -203,7 +211,7 @@ int cz_next_done(cz_server *s, int32_t timeout_ms, uint64_t *request_id);
  * is kept). */
 int cz_poll(cz_server *s, uint64_t request_id, int32_t timeout_ms, uint32_t *primes_out, uint32_t primes_cap,
             uint32_t *n_primes, cz_profile *out, uint32_t out_cap, uint32_t *n_profiles, uint32_t *a4_out);
-/* batches run, requests completed, requests waiting */
+/* filter launches so far, requests completed, requests waiting */
 int cz_server_info(cz_server *s, uint64_t *batches, uint64_t *completed, uint64_t *waiting);
 const char *cz_server_last_error(cz_server *s);
 

@@ -274,7 +274,7 @@ void admit(cz_server *s) {
     // not fit now waits, with everything behind it, for space to free up
     auto no_room = [&](CzRequest *r) {
         if (s->inflight.empty() && s->deferred.empty() && admitted.empty())
-            finish(s, r, CZ_ELIMIT, "request exceeds the server's prime, profile or plane capacity");
+            finish(s, r, CZ_EREFUSED, "refused: the request exceeds the server's prime, profile or plane capacity");
         else
             back.push_back(r);
     };
@@ -320,7 +320,7 @@ void admit(cz_server *s) {
         if (np) {
             u64 pb = 0, gb = 0, wb = 0, sl = 0;
             if (words > s->plane_words) {
-                finish(s, r, CZ_ELIMIT, "request's colour planes exceed the server's plane budget");
+                finish(s, r, CZ_EREFUSED, "refused: the request's colour planes exceed the server's plane budget");
                 continue;
             }
             if (!s->rp.alloc(np, pb)) { no_room(r); continue; }

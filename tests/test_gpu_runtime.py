@@ -117,3 +117,37 @@ def test_server_sieved_requests_and_next_done(eng):
         assert srv.batches >= 1
     finally:
         srv.close()
+
+
+def test_server_tight_plane_budget(eng):
+    """Admission by device memory: with a 96 MiB plane budget, a request whose
+    colour planes alone exceed it is refused (CZ_EREFUSED), while requests
+    that fit only one or two at a time are all served (they wait for space),
+    with records equal to cz_census's."""
+    from rabung_atlas32_b200 import _lib
+    from rabung_atlas32_b200.census import to_records
+    L, h = _server(slots=1, budget_mb=96)
+    try:
+        big = sieve.primes_ending(4294967291, 200)          # ~200 x 2 MiB of planes near 2^32
+        small = [sieve.primes_ending(4294967291 - k * 10 ** 6, 16) for k in range(6)]
+        ids = []
+        for ps in [big] + small:
+            arr = (ctypes.c_uint32 * len(ps))(*ps)
+            rid = ctypes.c_uint64()
+            assert L.cz_submit(h, 0, len(ps), arr, _lib.CZ_AUTO | _lib.CZ_A4, ctypes.byref(rid)) == _lib.CZ_OK
+            ids.append((rid.value, ps))
+        for rid, ps in ids:
+            out = (_lib.cz_profile * (8 * len(ps)))()
+            a4 = (ctypes.c_uint32 * len(ps))()
+            npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
+            rc = L.cz_poll(h, rid, 120000, None, 0, ctypes.byref(npr), out, 8 * len(ps), ctypes.byref(nprof), a4)
+            if ps is big:
+                assert rc == _lib.CZ_EREFUSED and b"plane budget" in L.cz_server_last_error(h)
+                continue
+            assert rc == _lib.CZ_OK
+            recs = to_records(ps, out, list(a4[:len(ps)]))
+            alone = eng.profiles(ps, mode="auto", a4=True)
+            assert [(r.p, [(v.r, v.M, v.L, v.witness, v.K) for v in r.profiles], r.a4) for r in recs] == \
+                   [(r.p, [(v.r, v.M, v.L, v.witness, v.K) for v in r.profiles], r.a4) for r in alone]
+    finally:
+        L.cz_server_close(h)

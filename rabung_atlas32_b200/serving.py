@@ -2,19 +2,17 @@
 
 A request asks for the profiles (and A4) of the `count` consecutive primes
 starting at `lo`.  `Server` drives the library's native serving runtime
-(cz_server_open / cz_submit / cz_next_done / cz_poll, csrc/runtime.cuh), which
-keeps every request's state resident until it is polled and runs continuous
-batching over `slots` in-flight batches (one library handle, hence one CUDA
-stream and one worker thread, per slot):
+(cz_server_open / cz_submit / cz_next_done / cz_poll, csrc/runtime.cuh):
 
-  * whenever a slot is free, every waiting request that fits is admitted into
-    one batch -- admission by device memory: the batch's colour-plane pool must
-    fit the slot's budget and the GPU's free memory (cz_mem_info);
-  * the batch's intervals are sieved on the device (cz_sieve), merged into one
-    census call (one persistent filter launch over all their profiles), and the
-    records are split back per request;
-  * requests that arrive while batches run wait for the next free slot, so work
-    of different batches overlaps on the device.
+  * every admitted request stays resident on the GPU (descriptors, state,
+    colour planes, records) until its records are final; admission is by free
+    colour-plane memory and descriptor space;
+  * the anchor filter is one persistent kernel over the unfinished profiles of
+    all admitted requests; an arrival makes it yield between work items, the
+    arrival is sieved, planned and tabled on the device, and the kernel is
+    relaunched over old and new profiles together -- requests join the work in
+    flight instead of waiting for a batch to end;
+  * a request's records are copied out as soon as its last profile is final.
 
 The reference has no serving path (its supervisor feeds fixed blocks to
 worker processes, src/census/worker32.cu:10-45); the records are the same as
@@ -59,10 +57,8 @@ def make_trace(n: int, rate: float, seed: int = 20261203) -> list:
 
 
 class Server:
-    """Continuous batching server: the library's native serving runtime
-    (cz_server_open / cz_submit / cz_next_done / cz_poll) with `slots` slots,
-    each with its own handle and CUDA stream and a slot budget for the colour-
-    plane pools of one batch."""
+    """The library's native serving runtime (cz_server_open / cz_submit /
+    cz_next_done / cz_poll); its colour-plane memory is slots x slot_budget_mb."""
 
     def __init__(self, slots: int = 2, slot_budget_mb: int = 16 * 1024, device: int = 0,
                  tuning: Tuning | None = None):
@@ -85,7 +81,7 @@ class Server:
 
     @property
     def batches(self) -> int:
-        """Batches run so far (the final count once the server is closed)."""
+        """Filter launches so far (the final count once the server is closed)."""
         if self.h is None:
             return self._closed_batches
         b = self._ct.c_uint64()
@@ -200,7 +196,7 @@ def benchmark(requests: int = 10000, rate: float = 40.0, seed: int = 20261203, s
     finally:
         srv.close()
     out = {"metric": "serving: p50/p99 latency and profiles/s", "offered_rate_rps": rate, "seed": seed,
-           "slots": slots, "batches": srv.batches, "continuous": summarize(served)}
+           "slots": slots, "filter_launches": srv.batches, "continuous": summarize(served)}
     if plain:
         ptrace = make_trace(requests, rate, seed)
         out["plain_per_request"] = summarize(serve_plain(ptrace))

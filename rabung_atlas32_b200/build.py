@@ -39,21 +39,27 @@ def source_key(extra=()) -> str:
     return h.hexdigest()
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    key = source_key()
-    if LIB.exists() and not force and KEY.exists() and KEY.read_text().strip() == key:
-        return LIB
-    tmp = LIB.with_suffix(f".{os.getpid()}.tmp.so")
-    cmd = [NVCC, *FLAGS, "-I", str(ROOT / "include"), "-o", str(tmp), str(CSRC / "census.cu"),
+def compile_library(out: Path, extra=(), verbose: bool = False) -> None:
+    """nvcc both translation units (32-bit and 33-bit prime words) into one
+    shared library at `out`; `extra` adds flags (e.g. -D build macros)."""
+    cmd = [NVCC, *FLAGS, *extra, "-I", str(ROOT / "include"), "-o", str(out), str(CSRC / "census.cu"),
            str(CSRC / "census_wide.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed for librabung_census.so")
+        raise RuntimeError(f"nvcc failed for {out.name}")
     if verbose:
         sys.stderr.write(r.stderr)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    key = source_key()
+    if LIB.exists() and not force and KEY.exists() and KEY.read_text().strip() == key:
+        return LIB
+    tmp = LIB.with_suffix(f".{os.getpid()}.tmp.so")
+    compile_library(tmp, verbose=verbose)
     os.replace(tmp, LIB)
     KEY.write_text(key + "\n")
     return LIB

@@ -91,9 +91,16 @@ struct CzRequest {
     std::vector<uint32_t> da4;
 };
 
+// the device ranges of one request, freed when no kernel can touch them
+struct Held {
+    u64 pbase, np, gbase, ng, wbase, nw;
+    u32 slot;
+};
+
 constexpr u32 SRV_CAP_PRIMES = 1u << 20;       // resident primes
 constexpr u32 SRV_CAP_PROFILES = 1u << 22;     // resident profiles
 constexpr u32 SRV_CAP_SLOTS = 1u << 16;        // requests in flight
+constexpr int SRV_MIN_LAUNCH_US = 5000;        // a launch runs this long before it yields to arrivals
 
 }  // namespace
 
@@ -114,7 +121,10 @@ struct cz_server {
     cudaStream_t cst = nullptr;                 // copies while the filter runs
     cudaEvent_t ev_kernel = nullptr;
     bool running = false, yielding = false;
-    std::vector<CzRequest *> inflight, deferred, repair;
+    bool blocked = false;                       // the oldest waiting request needs space in-flight work holds
+    std::chrono::steady_clock::time_point launch_t0;
+    std::vector<CzRequest *> inflight, repair;
+    std::vector<Held> deferred;                 // ranges of requests finished during the running launch
     std::thread sched;
     std::mutex m;
     std::condition_variable cv_work, cv_done;
@@ -128,23 +138,32 @@ struct cz_server {
 
 namespace {
 
+// publish a request's outcome; once it is announced the caller may release
+// it (cz_poll deletes it), so the scheduler must not touch r afterwards
 void finish(cz_server *s, CzRequest *r, int rc, const std::string &err = "") {
-    r->rc = rc;
-    r->err = err;
-    if (rc) { r->recs.clear(); r->a4.clear(); }
     {
         std::lock_guard<std::mutex> lk(s->m);
+        r->rc = rc;
+        r->err = err;
+        if (rc) { r->recs.clear(); r->a4.clear(); }
         s->announced.push_back(r->id);
         ++s->completed;
     }
     s->cv_done.notify_all();
 }
 
+Held held(const CzRequest *r) { return Held{r->pbase, r->np, r->gbase, r->ng, r->wbase, r->nw, r->slot}; }
+
+void release(cz_server *s, const Held &h) {
+    s->rp.release(h.pbase, h.np);
+    s->rg.release(h.gbase, h.ng);
+    s->rw.release(h.wbase, h.nw);
+    if (h.slot != 0xFFFFFFFFu) s->rs.release(h.slot, 1);
+}
+
+// ranges of a request no kernel is running for (admission window only)
 void release(cz_server *s, CzRequest *r) {
-    s->rp.release(r->pbase, r->np);
-    s->rg.release(r->gbase, r->ng);
-    s->rw.release(r->wbase, r->nw);
-    if (r->slot != 0xFFFFFFFFu) s->rs.release(r->slot, 1);
+    release(s, held(r));
     r->np = r->ng = r->nw = 0;
     r->slot = 0xFFFFFFFFu;
 }
@@ -230,8 +249,9 @@ void poll_done(cz_server *s) {
         s->inflight.erase(s->inflight.begin() + i);
         std::vector<u32> redo;
         const int rc = assemble(s, r, &redo);
-        s->deferred.push_back(r);                       // its ranges are freed after this launch
-        if (rc) { finish(s, r, rc, r->err.empty() ? std::string("record copy failed") : r->err); continue; }
+        s->deferred.push_back(held(r));                 // its ranges are freed after this launch
+        s->blocked = false;                             // its space frees when this launch ends
+        if (rc) { finish(s, r, rc, r->err.empty() ? std::string("record copy failed") : r->err); continue; }                             // its space frees when this launch ends
         if (!redo.empty()) { s->repair.push_back(r); continue; }
         finish(s, r, CZ_OK);
     }
@@ -400,6 +420,7 @@ void admit(cz_server *s) {
             s->inflight.clear();
         }
     }
+    s->blocked = !back.empty();
     if (!back.empty()) {
         std::lock_guard<std::mutex> lk(s->m);
         for (auto it = back.rbegin(); it != back.rend(); ++it) s->waiting.push_front(*it);
@@ -449,7 +470,11 @@ void sched_loop(cz_server *s) {
             stopping = s->stop;
         }
         if (s->running) {
-            if ((have_waiting || stopping || !s->repair.empty()) && !s->yielding) {
+            // yield to arrivals (unless the oldest waits for space still held)
+            // and to dense re-runs, once the launch has run its minimum time
+            const bool ripe = std::chrono::steady_clock::now() - s->launch_t0 >=
+                              std::chrono::microseconds(SRV_MIN_LAUNCH_US);
+            if ((stopping || (ripe && ((have_waiting && !s->blocked) || !s->repair.empty()))) && !s->yielding) {
                 cudaMemcpyAsync(s->d_yield, &s->h_flag[0], 4, cudaMemcpyHostToDevice, s->cst);
                 s->yielding = true;
             }
@@ -463,14 +488,14 @@ void sched_loop(cz_server *s) {
             poll_done(s);
             if (!s->yielding) {                        // a launch that ran to its end finished every profile
                 for (CzRequest *r : s->inflight) {
-                    s->deferred.push_back(r);
+                    s->deferred.push_back(held(r));
                     finish(s, r, CZ_EREFUSED, "refused: a profile did not finish");
                 }
                 s->inflight.clear();
             }
             s->yielding = false;
         }
-        for (CzRequest *r : s->deferred) release(s, r);
+        for (const Held &h : s->deferred) release(s, h);
         s->deferred.clear();
         if (stopping) return;
         run_repairs(s);
@@ -479,6 +504,7 @@ void sched_loop(cz_server *s) {
             launch(s);
             cudaEventRecord(s->ev_kernel, s->h->st);
             s->running = true;
+            s->launch_t0 = std::chrono::steady_clock::now();
             std::lock_guard<std::mutex> lk(s->m);
             ++s->launches;
             continue;

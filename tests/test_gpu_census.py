@@ -266,16 +266,13 @@ def test_small_tiles_do_not_change_records(tmp_path):
     every view into many tiles (up to ~20 per view here), so bands, halos and
     tile edges are crossed everywhere; its records must equal the default
     build's, with no prime sent back to the dense path."""
-    import subprocess
     from rabung_atlas32_b200 import _lib, build
     from rabung_atlas32_b200.census import Census, Tuning
     ps = sieve.primes_from(1 << 26, 40) + sieve.primes_from(1 << 28, 40) + sieve.primes_ending(1 << 30, 24)
     with Census(tuning=Tuning()) as c0:
         want = tup(c0.profiles(ps, mode="sparse", a4=False))
     so = tmp_path / "librabung_census_tile4k.so"
-    cmd = [build.NVCC, *build.FLAGS, "-DCZ_TILE_WORDS=4096", "-I", str(build.ROOT / "include"), "-o", str(so),
-           str(build.CSRC / "census.cu")]
-    subprocess.run(cmd, check=True, capture_output=True)
+    build.compile_library(so, extra=["-DCZ_TILE_WORDS=4096"])
     lib = _lib.load(so)
     saved = _lib._lib
     try:

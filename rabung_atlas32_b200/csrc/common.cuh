@@ -124,6 +124,21 @@ CZ_HD int top_bit(u64 e) {
 #endif
 }
 
+// two left-to-right binary powers with one exponent, interleaved: two
+// independent multiply chains per thread
+CZ_HD void mpow2(pw_t a, pw_t b, pw_t e, const Mont &M, pw_t &ra, pw_t &rb) {
+    if (e == 0) { ra = rb = M.one; return; }
+    const int top = top_bit(e);
+    pw_t va = a, vb = b;
+    for (int i = top - 1; i >= 0; --i) {
+        va = mmul(va, va, M);
+        vb = mmul(vb, vb, M);
+        if ((e >> i) & 1u) { va = mmul(va, a, M); vb = mmul(vb, b, M); }
+    }
+    ra = va;
+    rb = vb;
+}
+
 // left-to-right binary power of a Montgomery residue
 CZ_HD pw_t mpow(pw_t a, pw_t e, const Mont &M) {
     if (e == 0) return M.one;

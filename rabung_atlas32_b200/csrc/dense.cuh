@@ -128,17 +128,11 @@ dense_scan_kernel(DenseArgs a) {
         u32 bad = 0;
         if (active) {
             const u32 nsteps = (seg_end - seg_start) / 32u + 1u;
-            for (u32 st = 0; st < nsteps; ++st) {
+            // the run bookkeeping of one 32-wide step for every profile
+            auto step_runs = [&](u32 st, u32 label) {
                 const u32 base = seg_start + st * 32u;
-                const u32 x = base + lane;
-                const bool valid = x <= seg_end;
+                const bool valid = base + (u32)lane <= seg_end;
                 const u32 nvalid = min(32u, seg_end - base + 1u);
-                u32 label = 0;
-                if (valid) {
-                    const pw_t y = mpow(to_mont((pw_t)x, M), P.e, M);
-                    label = lookup_label(keys, labs, slots, y);
-                    if (label == 0xFFFFu) { bad = 1; label = 0; }
-                }
                 for (u32 s = 0; s < nprof; ++s) {
                     DRun R = drun[warp][s];
                     const u32 c = mod_small(label, R.r, R.mg);
@@ -195,6 +189,22 @@ dense_scan_kernel(DenseArgs a) {
                     drun[warp][s] = R;                     // every lane writes the same record
                     __syncwarp();
                 }
+            };
+            // labels two steps at a time: each lane's two powers are independent chains
+            auto label_of = [&](pw_t y, bool valid) {
+                if (!valid) return 0u;
+                u32 l = lookup_label(keys, labs, slots, y);
+                if (l == 0xFFFFu) { bad = 1; l = 0; }
+                return l;
+            };
+            for (u32 st = 0; st < nsteps; st += 2u) {
+                const u32 x0 = seg_start + st * 32u + (u32)lane, x1 = x0 + 32u;
+                const bool v0 = x0 <= seg_end, v1 = st + 1u < nsteps && x1 <= seg_end;
+                pw_t y0, y1;
+                mpow2(to_mont((pw_t)(v0 ? x0 : 1u), M), to_mont((pw_t)(v1 ? x1 : 1u), M), P.e, M, y0, y1);
+                const u32 l0 = label_of(y0, v0), l1 = label_of(y1, v1);
+                step_runs(st, l0);
+                if (st + 1u < nsteps) step_runs(st + 1u, l1);
             }
         }
         bad = __reduce_or_sync(0xFFFFFFFFu, bad);

@@ -475,7 +475,8 @@ def main():
             from rabung_atlas32_b200 import serving
             ck = ClockSampler(local)
             ck.start()
-            c5 = serving.benchmark(requests=args.requests, rate=args.rate, seed=20261203)
+            c5 = serving.benchmark(requests=args.requests, rate=args.rate, seed=20261203,
+                                   plain_requests=min(args.requests, 2000))
             c5["clocks"] = ck.stop()
             out["c5"] = c5
         print(json.dumps(out), flush=True)

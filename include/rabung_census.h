@@ -188,9 +188,11 @@ int cz_census_interval(cz_handle *h, uint64_t lo, uint64_t hi, uint32_t flags, u
  * finish a profile certifies and writes its record; a request's records are
  * copied out as soon as its last profile is final.  Primes below the sparse
  * route (small p) and dense re-runs use a second handle between launches;
- * speculative thresholds are off (records are unchanged by them).  A refusal
- * reaches only the request that caused it; a request whose colour planes
- * exceed the server's whole plane budget is refused.  Submit and poll may be
+ * speculative thresholds are off (records are unchanged by them).  A request
+ * whose colour planes exceed the server's whole plane budget runs on the
+ * second handle in waves of at most one slot's planes; a caller's non-prime is
+ * refused before any device work.  A refusal reaches only the request that
+ * caused it.  Submit and poll may be
  * called from any host thread.  The reference has no serving path; the
  * records equal cz_census's for the same primes. */
 typedef struct cz_server cz_server;

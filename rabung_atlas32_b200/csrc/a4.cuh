@@ -123,6 +123,10 @@ a4_kernel(const PrimeDesc *primes, u32 n, u32 *out, u32 *err) {
     if (idx >= n) return;
     const pw_t p = primes[idx].p;
     if (p <= 3u) { if (lane == 0) out[idx] = 0u; return; }
+    if (primes[idx].status & ST_ROOT) {           // not a prime (setup): no count, the call is refused
+        if (lane == 0) { atomicOr(err, 1u); out[idx] = 0u; }
+        return;
+    }
     const Mont M = make_mont(p);
     if (p < 1000u) {
         // direct count, characters by Euler's criterion

@@ -669,14 +669,15 @@ int census_impl(CZ_HANDLE *h, const pw_t *primes, uint32_t n, uint32_t flags, CZ
         if (h->nprof) cudaMemcpy(hs.data(), h->b_state.p, sizeof(ProfState) * h->nprof, cudaMemcpyDeviceToHost);
         for (auto &x : hs) { s.words += x.words; s.completions += x.completions; s.tests += x.tests; }
     }
+    // records first: a refusal names the prime and its status
+    std::vector<u32> fb, rs;
+    rc = check_records(h, allow_fallback ? &fb : nullptr, allow_fallback ? &rs : nullptr);
+    if (rc) return rc;
     if (flags & CZ_A4) {
         u32 a4err = 0;
         cudaMemcpy(&a4err, P<u32>(h->b_counter) + 8, 4, cudaMemcpyDeviceToHost);
         if (a4err) { h->err = "refused: A4 point count not certified"; return CZ_EREFUSED; }
     }
-    std::vector<u32> fb, rs;
-    rc = check_records(h, allow_fallback ? &fb : nullptr, allow_fallback ? &rs : nullptr);
-    if (rc) return rc;
     for (u32 g = 0; g < h->nprof; ++g) {
         const OutRecord &o = h->hout[g];
         CZ_RECORD &d = out[g];

@@ -15,8 +15,9 @@
 namespace CZ_NS {
 
 // deterministic Miller-Rabin with bases 2, 3, 5, 7, 11: no strong pseudoprime
-// to all five below 2.15e12, so exact for every n < 2^33
-__device__ inline bool is_prime_word(pw_t n) {
+// to all five below 2.15e12, so exact for every n < 2^33 (host and device:
+// the serving runtime refuses a caller's non-prime before any device work)
+__host__ __device__ inline bool is_prime_word(pw_t n) {
     if (n < 2u) return false;
     const u32 bases[5] = {2, 3, 5, 7, 11};
     for (int i = 0; i < 5; ++i) {

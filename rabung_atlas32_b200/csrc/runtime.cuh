@@ -21,9 +21,11 @@
 //    flag in mapped host memory, and the scheduler copies its records out
 //    while the kernel keeps running;
 //  * primes routed to the dense scan (small p), primes whose sparse record
-//    needs the dense re-run, and refusals are handled by a second handle in
-//    the window between launches; speculative thresholds are off here (a miss
-//    would need a re-run), which changes no record.
+//    needs the dense re-run, and requests larger than the whole plane arena
+//    (in waves of one slot's planes) are handled by a second handle in the
+//    window between launches; a caller's non-prime is refused on the host;
+//    speculative thresholds are off here (a miss would need a re-run), which
+//    changes no record.
 #pragma once
 #include <chrono>
 #include <condition_variable>
@@ -311,6 +313,18 @@ void admit(cz_server *s) {
         }
         const u32 n = (u32)r->primes.size();
         if (n == 0) { r->recs.clear(); r->a4.clear(); finish(s, r, CZ_OK); continue; }
+        if (r->given) {
+            // a caller's non-prime is refused here: on the filter it would
+            // match every window and run without a speculative threshold
+            u32 bad = 0;
+            bool composite = false;
+            for (u32 p : r->primes)
+                if (p > 2u && !is_prime_word(p)) { bad = p; composite = true; break; }
+            if (composite) {
+                finish(s, r, CZ_EREFUSED, "refused: p=" + std::to_string(bad) + " is not prime");
+                continue;
+            }
+        }
         u32 mode = r->flags & CZ_AUTO;
         if (!mode) mode = CZ_AUTO;
         int rc = plan(s->aux, r->primes.data(), n, mode | CZ_NOSPEC);
@@ -337,12 +351,15 @@ void admit(cz_server *s) {
         for (u32 i = 0; i < n; ++i) np += r->sparse[i];
         u64 ng = 0;
         for (u32 i = 0; i < n; ++i) if (r->sparse[i]) ng += s->aux->hp[i].nprof;
+        // a request larger than the whole resident arena runs on the second
+        // handle, in waves of at most one slot's planes, in this window
+        const bool oversize = words > s->plane_words || np > SRV_CAP_PRIMES || ng > SRV_CAP_PROFILES;
+        if (oversize) {
+            r->sparse.assign(n, 0u);
+            np = ng = 0;
+        }
         if (np) {
             u64 pb = 0, gb = 0, wb = 0, sl = 0;
-            if (words > s->plane_words) {
-                finish(s, r, CZ_EREFUSED, "refused: the request's colour planes exceed the server's plane budget");
-                continue;
-            }
             if (!s->rp.alloc(np, pb)) { no_room(r); continue; }
             if (!s->rg.alloc(ng, gb)) { s->rp.release(pb, np); no_room(r); continue; }
             if (!s->rw.alloc(words, wb)) { s->rp.release(pb, np); s->rg.release(gb, ng); no_room(r); continue; }
@@ -387,10 +404,11 @@ void admit(cz_server *s) {
             pend_slot.push_back((u32)sl);
             pend_val.push_back((u32)ng);
         }
-        // the other primes on the second handle (dense scan), in prime order
+        // the other primes on the second handle, in prime order: the dense
+        // scan, or the whole oversize request in its own mode
         std::vector<uint32_t> other;
         for (u32 i = 0; i < n; ++i) if (!r->sparse[i]) other.push_back(r->primes[i]);
-        rc = census_into(s->aux, other, (r->flags & ~CZ_AUTO) | CZ_DENSE, r->drecs, r->da4);
+        rc = census_into(s->aux, other, oversize ? r->flags : ((r->flags & ~CZ_AUTO) | CZ_DENSE), r->drecs, r->da4);
         if (rc) { release(s, r); finish(s, r, rc, cz_last_error(s->aux)); continue; }
         if (!np) {
             const int arc = assemble(s, r, nullptr);
@@ -586,11 +604,14 @@ int cz_server_open(const cz_config *cfg, uint32_t slots, uint64_t slot_budget_by
     cz_server *s = new cz_server();
     if (cfg) s->cfg = *cfg; else cz_default_config(&s->cfg);
     s->cfg.speculate = 0;                       // a speculative miss would need a re-run
+    const u64 per = slot_budget_bytes ? slot_budget_bytes : ((u64)s->cfg.plane_budget_mb << 20);
+    // the second handle's waves (oversize requests) hold at most one slot's planes
+    cz_config acfg = s->cfg;
+    acfg.plane_budget_mb = (uint32_t)std::max<u64>(64, std::min<u64>(acfg.plane_budget_mb, per >> 20));
     int rc = cz_open(&s->cfg, &s->h);
-    if (!rc) rc = cz_open(&s->cfg, &s->aux);
+    if (!rc) rc = cz_open(&acfg, &s->aux);
     if (rc) { server_free(s); return rc; }
     cudaSetDevice(s->h->dev);
-    const u64 per = slot_budget_bytes ? slot_budget_bytes : ((u64)s->cfg.plane_budget_mb << 20);
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     const u64 fixed = (u64)SRV_CAP_PRIMES * (sizeof(PrimeDesc) + 8) +

@@ -691,6 +691,7 @@ __device__ __noinline__ void load_profile(const SparseArgs &a, u32 gprof, ProfCt
     c.tpref = PD.tpref;
     c.tmax = c.tpref < 2u ? 2u : c.tpref;
     if (!plan_tiles(c, a.epoch_rows ? a.epoch_rows : EPOCH_ROWS_DEFAULT)) { c.nitems = 0; *err |= 4u; }
+    if (PR.status & ST_ROOT) c.nitems = 0;     // setup found no root (a non-prime): no work, its record is refused
     *out = c;
 }
 

@@ -78,6 +78,7 @@ table_kernel(TableArgs a) {
     for (u32 it = blockIdx.x; it < a.nsparse; it += gridDim.x) {
         const u32 pi = a.sparse_primes[it];
         const PrimeDesc P = a.primes[pi];
+        if (P.status & ST_ROOT) continue;   // not a prime, or no root of order m: the filter skips it
         const Mont M{P.p, P.ninv, P.one, P.r2};
         const u32 slots = hash_slots(P.m);
         // shared layout: root hash keys (slots words), their labels (slots u16),

@@ -188,7 +188,10 @@ def summarize(reqs: list) -> dict:
 
 
 def benchmark(requests: int = 10000, rate: float = 40.0, seed: int = 20261203, slots: int = 2,
-              plain: bool = True) -> dict:
+              plain: bool = True, plain_requests: int | None = None) -> dict:
+    """The trace served continuously; then, for comparison, its first
+    `plain_requests` requests (all when None) at the same arrival times as
+    plain per-request calls, with their records checked equal."""
     trace = make_trace(requests, rate, seed)
     srv = Server(slots=slots)
     try:
@@ -198,8 +201,11 @@ def benchmark(requests: int = 10000, rate: float = 40.0, seed: int = 20261203, s
     out = {"metric": "serving: p50/p99 latency and profiles/s", "offered_rate_rps": rate, "seed": seed,
            "slots": slots, "filter_launches": srv.batches, "continuous": summarize(served)}
     if plain:
-        ptrace = make_trace(requests, rate, seed)
+        k = requests if plain_requests is None else min(requests, plain_requests)
+        ptrace = make_trace(requests, rate, seed)[:k]
         out["plain_per_request"] = summarize(serve_plain(ptrace))
+        out["plain_per_request"]["trace_prefix"] = k
+        out["continuous_same_prefix"] = summarize(served[:k])
         same = all([(x.p, [(v.r, v.M, v.L, v.witness) for v in x.profiles], x.a4) for x in a.records] ==
                    [(x.p, [(v.r, v.M, v.L, v.witness) for v in x.profiles], x.a4) for x in b.records]
                    for a, b in zip(served, ptrace))

@@ -155,9 +155,17 @@ def test_sparse_threshold_region_vs_oracle(eng):
 
 
 def test_refusal_on_composite(eng):
+    """A non-prime is refused, and cheaply: setup marks it, and the table,
+    filter and A4 kernels do no work for it (every colour window of a
+    non-prime would match, so filtering it runs for tens of seconds)."""
+    import time
     from rabung_atlas32_b200.census import CensusError
     with pytest.raises(CensusError):
         eng.profiles([4294967291, 4294967293], mode="sparse", a4=False)
+    t0 = time.perf_counter()
+    with pytest.raises(CensusError, match="status"):
+        eng.profiles(sieve.primes_from(1 << 25, 8) + [(1 << 25) + 1], mode="sparse", a4=True)
+    assert time.perf_counter() - t0 < 5.0
 
 
 def test_replay_bit_identical(eng):

@@ -80,7 +80,7 @@ def test_server_refusal_reaches_only_its_request(eng):
             npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
             rc = L.cz_poll(h, rid, 60000, got, len(ps), ctypes.byref(npr), out, 8 * len(ps), ctypes.byref(nprof), a4)
             if ps is bad:
-                assert rc != _lib.CZ_OK and L.cz_server_last_error(h)
+                assert rc == _lib.CZ_EREFUSED and b"not prime" in L.cz_server_last_error(h)
                 continue
             assert rc == _lib.CZ_OK and list(got[:npr.value]) == ps
             recs = to_records(ps, out, list(a4[:len(ps)]))
@@ -121,9 +121,9 @@ def test_server_sieved_requests_and_next_done(eng):
 
 def test_server_tight_plane_budget(eng):
     """Admission by device memory: with a 96 MiB plane budget, a request whose
-    colour planes alone exceed it is refused (CZ_EREFUSED), while requests
-    that fit only one or two at a time are all served (they wait for space),
-    with records equal to cz_census's."""
+    colour planes alone exceed it runs on the second handle in waves, while
+    requests that fit only one or two at a time wait for space; every record
+    equals cz_census's."""
     from rabung_atlas32_b200 import _lib
     from rabung_atlas32_b200.census import to_records
     L, h = _server(slots=1, budget_mb=96)
@@ -141,9 +141,6 @@ def test_server_tight_plane_budget(eng):
             a4 = (ctypes.c_uint32 * len(ps))()
             npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
             rc = L.cz_poll(h, rid, 120000, None, 0, ctypes.byref(npr), out, 8 * len(ps), ctypes.byref(nprof), a4)
-            if ps is big:
-                assert rc == _lib.CZ_EREFUSED and b"plane budget" in L.cz_server_last_error(h)
-                continue
             assert rc == _lib.CZ_OK
             recs = to_records(ps, out, list(a4[:len(ps)]))
             alone = eng.profiles(ps, mode="auto", a4=True)

@@ -140,7 +140,10 @@ def test_server_tight_plane_budget(eng):
             out = (_lib.cz_profile * (8 * len(ps)))()
             a4 = (ctypes.c_uint32 * len(ps))()
             npr, nprof = ctypes.c_uint32(), ctypes.c_uint32()
+            # A4's capacity is primes_cap: too small a one is CZ_ELIMIT and keeps the request
             rc = L.cz_poll(h, rid, 120000, None, 0, ctypes.byref(npr), out, 8 * len(ps), ctypes.byref(nprof), a4)
+            assert rc == _lib.CZ_ELIMIT and npr.value == len(ps)
+            rc = L.cz_poll(h, rid, 0, None, len(ps), ctypes.byref(npr), out, 8 * len(ps), ctypes.byref(nprof), a4)
             assert rc == _lib.CZ_OK
             recs = to_records(ps, out, list(a4[:len(ps)]))
             alone = eng.profiles(ps, mode="auto", a4=True)

@@ -113,7 +113,10 @@ dense_scan_kernel(DenseArgs a) {
         const u32 local_chunk = chunk - a.chunk_prefix[pi];
         const u32 nh = (u32)((P.p - 1u) >> 1);             // p < 2^33: fits 32 bits
         const u32 seg = local_chunk * DENSE_WARPS + warp;
-        const u32 seg_start = 1u + seg * a.seg;              // x of the first element
+        // x of the segment's first element; in 64 bits, since (p-1)/2 reaches
+        // 2^32 - 1 in 64-bit words and the chunk's last segments lie past it
+        const u64 seg_start64 = 1ull + (u64)seg * a.seg;
+        const u32 seg_start = (u32)seg_start64;
         const u32 nprof = P.nprof;
         // per-profile run state: warp-uniform, so it lives in this warp's shared
         // records (one read and one write per profile per 32 x) instead of
@@ -123,16 +126,19 @@ dense_scan_kernel(DenseArgs a) {
             drun[warp][lane] = DRun{r, magic_of(r), 0xFFFFFFFFu, seg_start, 0u, 0u, 0u, 0u, 0u, 1u, 0u, 0u};
         }
         __syncwarp();
-        const bool active = seg_start <= nh;
-        const u32 seg_end = active ? min(nh, seg_start + a.seg - 1u) : 0u;   // inclusive
+        const bool active = seg_start64 <= (u64)nh;
+        const u32 seg_end = active ? (u32)min((u64)nh, seg_start64 + a.seg - 1u) : 0u;   // inclusive
+        // x is compared through its offset in the segment: seg_start + offset
+        // may pass 2^32 - 1 beyond seg_end, the offset never wraps
+        const u32 seg_last = seg_end - seg_start;
         u32 bad = 0;
         if (active) {
             const u32 nsteps = (seg_end - seg_start) / 32u + 1u;
             // the run bookkeeping of one 32-wide step for every profile
             auto step_runs = [&](u32 st, u32 label) {
                 const u32 base = seg_start + st * 32u;
-                const bool valid = base + (u32)lane <= seg_end;
-                const u32 nvalid = min(32u, seg_end - base + 1u);
+                const bool valid = st * 32u + (u32)lane <= seg_last;
+                const u32 nvalid = min(32u, seg_last - st * 32u + 1u);
                 for (u32 s = 0; s < nprof; ++s) {
                     DRun R = drun[warp][s];
                     const u32 c = mod_small(label, R.r, R.mg);
@@ -198,8 +204,9 @@ dense_scan_kernel(DenseArgs a) {
                 return l;
             };
             for (u32 st = 0; st < nsteps; st += 2u) {
-                const u32 x0 = seg_start + st * 32u + (u32)lane, x1 = x0 + 32u;
-                const bool v0 = x0 <= seg_end, v1 = st + 1u < nsteps && x1 <= seg_end;
+                const u32 o0 = st * 32u + (u32)lane, o1 = o0 + 32u;
+                const bool v0 = o0 <= seg_last, v1 = st + 1u < nsteps && o1 <= seg_last;
+                const u32 x0 = seg_start + o0, x1 = seg_start + o1;
                 pw_t y0, y1;
                 mpow2(to_mont((pw_t)(v0 ? x0 : 1u), M), to_mont((pw_t)(v1 ? x1 : 1u), M), P.e, M, y0, y1);
                 const u32 l0 = label_of(y0, v0), l1 = label_of(y1, v1);

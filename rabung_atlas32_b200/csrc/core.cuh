@@ -250,8 +250,12 @@ int plan(CZ_HANDLE *h, const pw_t *primes, u32 n, u32 flags) {
         } else {
             const u32 nh = (u32)((p - 1u) / 2u);           // < 2^32 for p < 2^33
             const u32 seg = dense_seg(c);
-            const u32 nseg = (nh + seg - 1u) / seg;
+            const u32 nseg = (u32)(((u64)nh + seg - 1u) / seg);   // nh + seg wraps 32 bits near 2^33
             const u32 nch = (nseg + DENSE_WARPS - 1u) / DENSE_WARPS;
+            if ((u64)h->h_chunk.back() + nch > 0xFFFFFFFFull || summ_slots + (u64)nch * P.nprof > 0xFFFFFFFFull) {
+                h->err = "dense scan too large for one call (chunk index beyond 32 bits)";
+                return CZ_ELIMIT;
+            }
             h->h_didx.push_back(i);
             h->h_summp.push_back((u32)summ_slots);
             summ_slots += (u64)nch * P.nprof;

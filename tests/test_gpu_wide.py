@@ -74,7 +74,7 @@ def test_wide_refusals(wide):
     from rabung_atlas32_b200 import _lib
     from rabung_atlas32_b200.census import CensusError
     with pytest.raises(CensusError):
-        wide.profiles([5389000007, 5389000009], mode="sparse", a4=False)
+        wide.profiles([5389000007, 5389000013], mode="sparse", a4=False)   # 37 x 83 x 1754803
     lib = _lib.load()
     arr = (ctypes.c_uint64 * 1)(2 ** 33 + 17)
     out = (_lib.cz_profile64 * 8)()

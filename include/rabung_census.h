@@ -188,7 +188,8 @@ int cz_census_interval(cz_handle *h, uint64_t lo, uint64_t hi, uint32_t flags, u
  * finish a profile certifies and writes its record; a request's records are
  * copied out as soon as its last profile is final.  Primes below the sparse
  * route (small p) and dense re-runs use a second handle between launches;
- * speculative thresholds are off (records are unchanged by them).  A request
+ * a profile whose speculative threshold missed is re-run there without
+ * speculation, as cz_census does (records are unchanged by it).  A request
  * whose colour planes exceed the server's whole plane budget runs on the
  * second handle in waves of at most one slot's planes; a caller's non-prime is
  * refused before any device work.  A refusal reaches only the request that
@@ -215,6 +216,18 @@ int cz_poll(cz_server *s, uint64_t request_id, int32_t timeout_ms, uint32_t *pri
             uint32_t *n_primes, cz_profile *out, uint32_t out_cap, uint32_t *n_profiles, uint32_t *a4_out);
 /* filter launches so far, requests completed, requests waiting */
 int cz_server_info(cz_server *s, uint64_t *batches, uint64_t *completed, uint64_t *waiting);
+/* scheduler counters: filter launches, launches that yielded to arrivals or
+ * re-runs, requests completed and waiting, primes re-run without speculation
+ * (a speculative miss) and on the dense scan (other fallbacks), requests
+ * served in waves on the second handle (larger than the plane arena), and the
+ * milliseconds spent draining yielded launches (yield flag to kernel end) and
+ * in the windows between launches (kernel end to relaunch) */
+typedef struct cz_server_counters {
+    uint64_t launches, yields, completed, waiting;
+    uint64_t respec_primes, fallback_primes, oversize_requests;
+    double ms_drain, ms_window;
+} cz_server_counters;
+int cz_server_stats(cz_server *s, cz_server_counters *out);
 const char *cz_server_last_error(cz_server *s);
 
 /* ---- the 33-bit domain -------------------------------------------------------

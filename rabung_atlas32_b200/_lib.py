@@ -49,10 +49,20 @@ class cz_stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class cz_server_counters(ctypes.Structure):
+    _fields_ = [("launches", u64), ("yields", u64), ("completed", u64), ("waiting", u64),
+                ("respec_primes", u64), ("fallback_primes", u64), ("oversize_requests", u64),
+                ("ms_drain", ctypes.c_double), ("ms_window", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 EXPORTS = ["cz_default_config", "cz_open", "cz_close", "cz_last_error", "cz_count_profiles",
            "cz_census", "cz_replay", "cz_a4", "cz_sieve", "cz_plane_bytes", "cz_mem_info", "cz_device_info",
            "cz_microbench", "cz_census_dense_noalloc", "cz_census_interval", "cz_server_open",
-           "cz_server_close", "cz_submit", "cz_next_done", "cz_poll", "cz_server_info", "cz_server_last_error",
+           "cz_server_close", "cz_submit", "cz_next_done", "cz_poll", "cz_server_info", "cz_server_stats",
+           "cz_server_last_error",
            "cz_prime_count", "cz_open64", "cz_close64", "cz_last_error64", "cz_count_profiles64", "cz_census64",
            "baseline_init", "baseline_profile"]
 
@@ -116,6 +126,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.cz_poll.restype = ctypes.c_int
     L.cz_server_info.argtypes = [H, P64, P64, P64]
     L.cz_server_info.restype = ctypes.c_int
+    L.cz_server_stats.argtypes = [H, ctypes.POINTER(cz_server_counters)]
+    L.cz_server_stats.restype = ctypes.c_int
     L.cz_server_last_error.argtypes = [H]
     L.cz_server_last_error.restype = ctypes.c_char_p
     L.cz_open64.argtypes = [ctypes.POINTER(cz_config), ctypes.POINTER(H)]

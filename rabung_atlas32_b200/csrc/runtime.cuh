@@ -24,8 +24,8 @@
 //    needs the dense re-run, and requests larger than the whole plane arena
 //    (in waves of one slot's planes) are handled by a second handle in the
 //    window between launches; a caller's non-prime is refused on the host;
-//    speculative thresholds are off here (a miss would need a re-run), which
-//    changes no record.
+//    a profile whose speculative threshold missed is re-run there on the
+//    anchor filter without speculation, as cz_census does.
 #pragma once
 #include <chrono>
 #include <condition_variable>
@@ -124,7 +124,8 @@ struct cz_server {
     cudaEvent_t ev_kernel = nullptr;
     bool running = false, yielding = false;
     bool blocked = false;                       // the oldest waiting request needs space in-flight work holds
-    std::chrono::steady_clock::time_point launch_t0;
+    std::chrono::steady_clock::time_point launch_t0, t_yield, t_end;
+    bool ended = false;                         // a launch ended and the next has not started
     std::vector<CzRequest *> inflight, repair;
     std::vector<Held> deferred;                 // ranges of requests finished during the running launch
     std::thread sched;
@@ -134,6 +135,8 @@ struct cz_server {
     std::unordered_map<uint64_t, CzRequest *> reqs;
     std::deque<uint64_t> announced;     // completed, not yet returned by cz_next_done
     uint64_t next_id = 1, launches = 0, completed = 0;
+    uint64_t yields = 0, n_respec = 0, n_fallback = 0, n_oversize = 0;
+    double ms_drain = 0, ms_window = 0;         // yield flag -> kernel end; kernel end -> relaunch
     bool stop = false;
     std::string err;
 };
@@ -219,27 +222,50 @@ int assemble(cz_server *s, CzRequest *r, std::vector<uint32_t> *redo) {
     return CZ_OK;
 }
 
-// dense re-run of the primes of r listed in redo (indices into r->primes),
-// patching their records in place (the window between launches only)
+// re-run of the primes of r listed in redo (indices into r->primes) on the
+// second handle, patching their records in place (the window between
+// launches only): a prime whose only fault is a speculative miss (its best
+// run stayed below the speculative threshold) runs on the anchor filter
+// without speculation; any other fallback status runs on the dense scan
 int repair(cz_server *s, CzRequest *r, const std::vector<u32> &redo) {
-    std::vector<u32> ps, first;
     size_t off = 0;
     std::vector<size_t> start(r->primes.size());
     for (size_t i = 0; i < r->primes.size(); ++i) {
         start[i] = off;
         off += r->primes[i] > 2u ? popc(mask_of(r->primes[i])) : 0u;
     }
-    for (u32 i : redo) ps.push_back(r->primes[i]);
-    std::vector<cz_profile> recs;
-    std::vector<uint32_t> a4;
-    const int rc = census_into(s->aux, ps, (r->flags & ~(CZ_AUTO | CZ_A4)) | CZ_DENSE, recs, a4);
-    if (rc) { r->err = cz_last_error(s->aux); return rc; }
-    size_t t = 0;
+    std::vector<u32> spec_i, dense_i;
     for (u32 i : redo) {
+        bool only_spec = true;
         const u32 k = popc(mask_of(r->primes[i]));
-        for (u32 j = 0; j < k; ++j) r->recs[start[i] + j] = recs[t++];
+        for (u32 j = 0; j < k; ++j)
+            if (r->recs[start[i] + j].status & ~ST_SPEC) only_spec = false;
+        (only_spec ? spec_i : dense_i).push_back(i);
     }
-    return CZ_OK;
+    auto rerun = [&](const std::vector<u32> &idx, uint32_t flags) -> int {
+        if (idx.empty()) return CZ_OK;
+        std::vector<u32> ps;
+        for (u32 i : idx) ps.push_back(r->primes[i]);
+        std::vector<cz_profile> recs;
+        std::vector<uint32_t> a4;
+        const int rc = census_into(s->aux, ps, flags, recs, a4);
+        if (rc) { r->err = cz_last_error(s->aux); return rc; }
+        size_t t = 0;
+        for (u32 i : idx) {
+            const u32 k = popc(mask_of(r->primes[i]));
+            for (u32 j = 0; j < k; ++j) r->recs[start[i] + j] = recs[t++];
+        }
+        return CZ_OK;
+    };
+    const uint32_t keep = r->flags & ~(CZ_AUTO | CZ_A4);
+    int rc = rerun(spec_i, keep | CZ_SPARSE | CZ_NOSPEC);
+    if (!rc) rc = rerun(dense_i, keep | CZ_DENSE);
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        s->n_respec += spec_i.size();
+        s->n_fallback += dense_i.size();
+    }
+    return rc;
 }
 
 // requests whose done flag is up: records out (while the filter runs), then
@@ -327,7 +353,7 @@ void admit(cz_server *s) {
         }
         u32 mode = r->flags & CZ_AUTO;
         if (!mode) mode = CZ_AUTO;
-        int rc = plan(s->aux, r->primes.data(), n, mode | CZ_NOSPEC);
+        int rc = plan(s->aux, r->primes.data(), n, mode);
         if (rc) { finish(s, r, rc, s->aux->err); continue; }
         // the resident (sparse) part of the plan
         std::vector<PrimeDesc> hp;
@@ -355,6 +381,10 @@ void admit(cz_server *s) {
         // handle, in waves of at most one slot's planes, in this window
         const bool oversize = words > s->plane_words || np > SRV_CAP_PRIMES || ng > SRV_CAP_PROFILES;
         if (oversize) {
+            {
+                std::lock_guard<std::mutex> lk(s->m);
+                ++s->n_oversize;
+            }
             r->sparse.assign(n, 0u);
             np = ng = 0;
         }
@@ -495,6 +525,7 @@ void sched_loop(cz_server *s) {
             if ((stopping || (ripe && ((have_waiting && !s->blocked) || !s->repair.empty()))) && !s->yielding) {
                 cudaMemcpyAsync(s->d_yield, &s->h_flag[0], 4, cudaMemcpyHostToDevice, s->cst);
                 s->yielding = true;
+                s->t_yield = std::chrono::steady_clock::now();
             }
             if (cudaEventQuery(s->ev_kernel) != cudaSuccess) {
                 std::unique_lock<std::mutex> lk(s->m);
@@ -503,6 +534,13 @@ void sched_loop(cz_server *s) {
             }
             cudaStreamSynchronize(s->cst);
             s->running = false;
+            s->t_end = std::chrono::steady_clock::now();
+            s->ended = true;
+            if (s->yielding) {
+                std::lock_guard<std::mutex> lk(s->m);
+                ++s->yields;
+                s->ms_drain += std::chrono::duration<double, std::milli>(s->t_end - s->t_yield).count();
+            }
             poll_done(s);
             if (!s->yielding) {                        // a launch that ran to its end finished every profile
                 for (CzRequest *r : s->inflight) {
@@ -525,8 +563,11 @@ void sched_loop(cz_server *s) {
             s->launch_t0 = std::chrono::steady_clock::now();
             std::lock_guard<std::mutex> lk(s->m);
             ++s->launches;
+            if (s->ended) s->ms_window += std::chrono::duration<double, std::milli>(s->launch_t0 - s->t_end).count();
+            s->ended = false;
             continue;
         }
+        s->ended = false;                              // idle: no window to count
         std::unique_lock<std::mutex> lk(s->m);
         s->cv_work.wait(lk, [s] { return s->stop || !s->waiting.empty(); });
     }
@@ -603,7 +644,6 @@ int cz_server_open(const cz_config *cfg, uint32_t slots, uint64_t slot_budget_by
     *out = nullptr;
     cz_server *s = new cz_server();
     if (cfg) s->cfg = *cfg; else cz_default_config(&s->cfg);
-    s->cfg.speculate = 0;                       // a speculative miss would need a re-run
     const u64 per = slot_budget_bytes ? slot_budget_bytes : ((u64)s->cfg.plane_budget_mb << 20);
     // the second handle's waves (oversize requests) hold at most one slot's planes
     cz_config acfg = s->cfg;
@@ -731,6 +771,22 @@ int cz_server_info(cz_server *s, uint64_t *batches, uint64_t *completed, uint64_
     if (batches) *batches = s->launches;
     if (completed) *completed = s->completed;
     if (waiting) *waiting = s->waiting.size();
+    return CZ_OK;
+}
+
+int cz_server_stats(cz_server *s, cz_server_counters *out) {
+    if (!s || !out) return CZ_EINVAL;
+    std::lock_guard<std::mutex> lk(s->m);
+    *out = cz_server_counters{};
+    out->launches = s->launches;
+    out->yields = s->yields;
+    out->completed = s->completed;
+    out->waiting = s->waiting.size();
+    out->respec_primes = s->n_respec;
+    out->fallback_primes = s->n_fallback;
+    out->oversize_requests = s->n_oversize;
+    out->ms_drain = s->ms_drain;
+    out->ms_window = s->ms_window;
     return CZ_OK;
 }
 

@@ -77,6 +77,7 @@ class Server:
             raise RuntimeError(f"cz_server_open failed (rc={rc})")
         self.h = h
         self._closed_batches = 0
+        self._closed_stats = {}
         self.t0 = 0.0
 
     @property
@@ -88,9 +89,18 @@ class Server:
         self.lib.cz_server_info(self.h, self._ct.byref(b), None, None)
         return int(b.value)
 
+    def stats(self) -> dict:
+        """Scheduler counters (cz_server_stats); the final ones once closed."""
+        if self.h is None:
+            return dict(self._closed_stats)
+        st = self._L.cz_server_counters()
+        self.lib.cz_server_stats(self.h, self._ct.byref(st))
+        return {k: (round(v, 1) if isinstance(v, float) else int(v)) for k, v in st.as_dict().items()}
+
     def close(self):
         if self.h is not None:
             self._closed_batches = self.batches
+            self._closed_stats = self.stats()
             self.lib.cz_server_close(self.h)
             self.h = None
 
@@ -199,7 +209,8 @@ def benchmark(requests: int = 10000, rate: float = 40.0, seed: int = 20261203, s
     finally:
         srv.close()
     out = {"metric": "serving: p50/p99 latency and profiles/s", "offered_rate_rps": rate, "seed": seed,
-           "slots": slots, "filter_launches": srv.batches, "continuous": summarize(served)}
+           "slots": slots, "filter_launches": srv.batches, "scheduler": srv.stats(),
+           "continuous": summarize(served)}
     if plain:
         k = requests if plain_requests is None else min(requests, plain_requests)
         ptrace = make_trace(requests, rate, seed)[:k]

@@ -151,3 +151,24 @@ def test_server_tight_plane_budget(eng):
                    [(r.p, [(v.r, v.M, v.L, v.witness, v.K) for v in r.profiles], r.a4) for r in alone]
     finally:
         L.cz_server_close(h)
+
+
+def test_server_speculation_misses_rerun_exact(eng):
+    """Speculative thresholds at floor(log_r p) (margin 0) miss often; the
+    server re-runs each missed prime on the anchor filter without speculation
+    (no dense re-scan), and every record equals cz_census's."""
+    from rabung_atlas32_b200.census import Tuning
+    from rabung_atlas32_b200.serving import Server
+    srv = Server(slots=1, slot_budget_mb=2048, tuning=Tuning(speculate=1, spec_margin10=(0,) * 10))
+    try:
+        reqs = [(4294967291 - 3 * 10 ** 6, 48), (1 << 31, 32)]
+        ids = {srv.submit(lo, n): (lo, n) for lo, n in reqs}
+        for rid, (lo, n) in ids.items():
+            primes, recs = srv.fetch(rid, n)
+            alone = eng.profiles(primes, mode="auto", a4=True)
+            assert [(r.p, [(v.r, v.M, v.L, v.witness, v.K) for v in r.profiles], r.a4) for r in recs] == \
+                   [(r.p, [(v.r, v.M, v.L, v.witness, v.K) for v in r.profiles], r.a4) for r in alone]
+        st = srv.stats()
+        assert st["respec_primes"] > 0
+    finally:
+        srv.close()

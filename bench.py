@@ -417,15 +417,20 @@ def main():
                                                                "ms_a4", "ms_finalize")},
                 "certification": "every record certified on the device in each step (finalize_kernel: witness "
                                  "run and its two ends by direct powers, prefix; its time is ms_finalize)"}
-        # DRAM traffic of one full-size sparse_kernel launch, from the committed
+        # traffic measured in this run: the colour-plane bytes the filter staged
+        # from global memory into shared memory (cp.async.bulk), counted in-kernel
+        roof["traffic"] = int(kstats["staged_bytes"])
+        roof["traffic_source"] = ("in-kernel count of plane bytes staged global -> shared by cp.async.bulk, "
+                                  "one launch (the screen's and completions' direct plane reads are not included)")
+        # for comparison: DRAM bytes of one full-size launch from the committed
         # ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum)
         prof_path = ROOT / "profiles" / "sparse_kernel_dram_top_block.txt"
         if prof_path.exists():
             for line in prof_path.read_text().splitlines():
                 if line.startswith("dram_bytes_per_launch:"):
                     try:
-                        roof["traffic"] = int(line.split(":")[1].split()[0])
-                        roof["traffic_source"] = "ncu, full 4096-prime launch (" + prof_path.name + ")"
+                        roof["traffic_ncu_dram"] = int(line.split(":")[1].split()[0])
+                        roof["traffic_ncu_source"] = prof_path.name
                     except ValueError:
                         pass
         # plain form: one prime per call (the reference worker's per-prime launches)

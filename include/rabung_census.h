@@ -85,6 +85,7 @@ typedef struct cz_stats {
     uint64_t words, completions;    /* sparse filter words visited, exact completions */
     uint64_t tests;                 /* plane-window comparisons executed by the filter */
     uint64_t h2d_bytes, d2h_bytes;
+    uint64_t staged_bytes;          /* colour-plane bytes the filter copied into shared memory */
 } cz_stats;
 
 typedef struct cz_handle cz_handle;

@@ -43,7 +43,7 @@ class cz_stats(ctypes.Structure):
                 ("n_primes", u32), ("n_dense", u32), ("n_sparse", u32), ("n_profiles", u32),
                 ("n_fallback", u32), ("n_respec", u32), ("ms_respec", ctypes.c_float), ("waves", u32),
                 ("kernels", u32), ("words", u64), ("completions", u64),
-                ("tests", u64), ("h2d_bytes", u64), ("d2h_bytes", u64)]
+                ("tests", u64), ("h2d_bytes", u64), ("d2h_bytes", u64), ("staged_bytes", u64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

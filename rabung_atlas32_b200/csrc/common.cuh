@@ -224,7 +224,7 @@ struct ProfState {
     u32 status;
     u32 active;               // serving: CTAs working on the profile now
     u32 done;                 // serving: 1 once its record is final
-    u32 pad;
+    u32 staged16;             // sparse filter: plane bytes staged into shared memory, / 16
     unsigned long long words;       // filter words visited
     unsigned long long completions; // exact completions run
     unsigned long long tests;       // plane-window comparisons (stage x plane) executed

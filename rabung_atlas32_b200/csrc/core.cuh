@@ -616,6 +616,7 @@ int census_waves(CZ_HANDLE *h, const pw_t *primes, uint32_t n, uint32_t flags, C
             tot.n_fallback += s.n_fallback; tot.n_respec += s.n_respec; tot.ms_respec += s.ms_respec;
             tot.kernels += s.kernels; tot.words += s.words; tot.completions += s.completions;
             tot.tests += s.tests; tot.h2d_bytes += s.h2d_bytes; tot.d2h_bytes += s.d2h_bytes;
+            tot.staged_bytes += s.staged_bytes;
             prof_off += np;
             start = i;
             acc = 0;
@@ -671,7 +672,10 @@ int census_impl(CZ_HANDLE *h, const pw_t *primes, uint32_t n, uint32_t flags, CZ
     {
         std::vector<ProfState> hs(h->nprof);
         if (h->nprof) cudaMemcpy(hs.data(), h->b_state.p, sizeof(ProfState) * h->nprof, cudaMemcpyDeviceToHost);
-        for (auto &x : hs) { s.words += x.words; s.completions += x.completions; s.tests += x.tests; }
+        for (auto &x : hs) {
+            s.words += x.words; s.completions += x.completions; s.tests += x.tests;
+            s.staged_bytes += 16ull * x.staged16;
+        }
     }
     // records first: a refusal names the prime and its status
     std::vector<u32> fb, rs;

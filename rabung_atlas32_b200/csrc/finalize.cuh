@@ -69,7 +69,7 @@ __global__ void setup_kernel(PrimeDesc *primes, ProfDesc *profs, ProfState *stat
             }
             ProfState &S = state[P.first_prof + s];
             S.best = 0; S.claim = 0; S.seed = 0; S.firstnz = 0xFFFFFFFFu;
-            S.status = 0; S.active = 0; S.done = 0; S.pad = 0; S.words = 0; S.completions = 0; S.tests = 0;
+            S.status = 0; S.active = 0; S.done = 0; S.staged16 = 0; S.words = 0; S.completions = 0; S.tests = 0;
         }
     }
     P.status = status;

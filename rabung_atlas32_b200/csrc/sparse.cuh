@@ -667,6 +667,7 @@ __device__ __noinline__ bool next_item(const ProfCtx &c, ProfState *st, u32 erow
     it.S = tile;
     it.ubase = 32u * w0;
     *out = it;
+    atomicAdd(&st->staged16, bytes >> 4);
     mbar_expect_tx(mbar, bytes);
     bulk_load(tile, v.P + (size_t)w0 * c.npp, bytes, mbar);
     return true;

@@ -65,7 +65,7 @@ typedef struct cz_config {
     uint32_t sparse_blocks;  /* persistent filter grid (0: 2 per SM) */
     uint32_t use_graph;      /* 1: replay device work through a captured CUDA graph */
     uint32_t cta_per_profile; /* CTAs sharing one profile's rows (L2 working set) */
-    uint32_t epoch_rows;     /* filter rows d per threshold epoch (0: 256; at most 2^20) */
+    uint32_t epoch_rows;     /* filter rows d per threshold epoch (0: 1024; at most 2^20) */
     uint32_t speculate;      /* 1: speculative thresholds floor(log_r p - margin), re-run on a miss */
     uint32_t spec_margin10[10];  /* margin per order r, in tenths */
     uint32_t plane_budget_mb;    /* plane pool per wave; larger batches run as consecutive waves */

@@ -82,7 +82,7 @@ def tune(quick: bool = False, log=print) -> dict:
     log(f"baseline sparse {ref_ms:.1f} ms")
     best = dataclasses.replace(base)
     best_ms = ref_ms
-    space = {"anchor_bits": [3, 4, 5], "cta_per_profile": [1, 2, 3, 4], "epoch_rows": [128, 256, 512],
+    space = {"anchor_bits": [3, 4, 5], "cta_per_profile": [1, 2, 3, 4], "epoch_rows": [256, 512, 1024, 2048],
              "cover_n": [3, 4]}
     rejected = []
     for _ in range(1 if quick else 2):

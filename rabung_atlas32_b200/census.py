@@ -37,7 +37,7 @@ class Tuning:
     sparse_blocks: int = 0
     use_graph: int = 1
     cta_per_profile: int = 2
-    epoch_rows: int = 256
+    epoch_rows: int = 1024
     speculate: int = 1
     spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 10, 0, 5, 10)
     plane_budget_mb: int = 24 * 1024

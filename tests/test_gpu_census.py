@@ -264,7 +264,7 @@ def test_epoch_rows_do_not_change_records():
     ps = sieve.primes_ending(4294967291, 48) + sieve.primes_from(1 << 24, 48)
     with Census(tuning=Tuning()) as c0:
         want = tup(c0.profiles(ps, mode="sparse", a4=False))
-    for er in (1, 7, 64, 1 << 20):
+    for er in (1, 7, 64, 256, 1 << 20):
         with Census(tuning=dataclasses.replace(Tuning(), epoch_rows=er)) as c1:
             assert tup(c1.profiles(ps, mode="sparse", a4=False)) == want, er
 

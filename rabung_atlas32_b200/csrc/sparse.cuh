@@ -166,7 +166,21 @@ struct View {
     u32 OFF;          // bit index of i = 0
     i32 ilo, ihi;
     u32 G, c;
+    u32 gs;           // log2 G: the view's divisions by G are shifts
 };
+
+// x / y from one float reciprocal ry = 1 / y (round to nearest): the
+// truncated product is within one of the quotient for x < 2^21 + 2 y (a
+// float32 emulation over the filter's ranges, y <= 2^28, confirms it), and the
+// remainder corrects it.  Every quotient of the row set-up is in that range:
+// numerators are at most 2^20 + step, ranks below 2^20.
+__device__ __forceinline__ u32 div_rcp(u32 x, u32 y, float ry) {
+    u32 q = __float2uint_rz(__uint2float_rn(x) * ry);
+    const i32 r = (i32)(x - q * y);
+    if (r < 0) --q;
+    else if ((u32)r >= y) ++q;
+    return q;
+}
 
 struct ProfCtx {
     pw_t p, ex;            // prime, (p - 1) / r
@@ -347,7 +361,7 @@ __device__ __forceinline__ void screen_batch(const ProfCtx &c, uint4 *sb, Cand *
         vc = v.c;
         vg = v.G;
         const u32 h = thr > t ? thr - t : 0u;     // reject runs certified < threshold
-        if (screen && h > 0u) keep = screen_word<NPP>(v, i0, keep, d / v.G, t, h);
+        if (screen && h > 0u) keep = screen_word<NPP>(v, i0, keep, d >> v.gs, t, h);
     }
     __syncwarp();
     // shift the rest down (up to SCR_CAP - 32 entries; each lane moves its own
@@ -432,42 +446,45 @@ __device__ __forceinline__ void bulk_load(u32 dst, const void *src, u32 bytes, u
                  :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
-// 64-bit window lo = bits [u, u+32), hi = bits [u+32, u+64) of the NPP
-// interleaved planes of a tile at shared byte address S (word w of plane k at
-// S + 4 (w NPP + k))
+// two 32-bit windows of the NPP interleaved planes of a tile at shared byte
+// address S (word w of plane k at S + 4 (w NPP + k)): lo = bits [u, u+32) and
+// hi = bits [u + 32 nb, u + 32 nb + 32), where offb = 4 NPP nb is the byte
+// distance of the two halves.  Both halves share the shift u mod 32; each
+// reads two consecutive words, so lanes holding consecutive words of a band
+// read consecutive shared addresses (no bank conflicts)
 template <int NPP> struct Tile;
 template <> struct Tile<1> {
-    static __device__ __forceinline__ void win64(u32 S, u32 u, u32 *lo, u32 *hi) {
-        const u32 a0 = S + 4u * (u >> 5), sh = u & 31u;
-        const u32 a = lds32(a0), b = lds32(a0 + 4u), c = lds32(a0 + 8u);
-        lo[0] = __funnelshift_r(a, b, sh);
-        hi[0] = __funnelshift_r(b, c, sh);
+    static __device__ __forceinline__ void win2(u32 S, u32 u, u32 offb, u32 *lo, u32 *hi) {
+        const u32 a = S + 4u * (u >> 5), b = a + offb;
+        const u32 a0 = lds32(a), a1 = lds32(a + 4u), b0 = lds32(b), b1 = lds32(b + 4u);
+        lo[0] = __funnelshift_r(a0, a1, u);
+        hi[0] = __funnelshift_r(b0, b1, u);
     }
 };
 template <> struct Tile<2> {
-    static __device__ __forceinline__ void win64(u32 S, u32 u, u32 *lo, u32 *hi) {
-        const u32 a0 = S + 8u * (u >> 5), sh = u & 31u;
-        const uint2 a = lds64(a0), b = lds64(a0 + 8u), c = lds64(a0 + 16u);
-        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
-        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
+    static __device__ __forceinline__ void win2(u32 S, u32 u, u32 offb, u32 *lo, u32 *hi) {
+        const u32 a = S + 8u * (u >> 5), b = a + offb;
+        const uint2 a0 = lds64(a), a1 = lds64(a + 8u), b0 = lds64(b), b1 = lds64(b + 8u);
+        lo[0] = __funnelshift_r(a0.x, a1.x, u); lo[1] = __funnelshift_r(a0.y, a1.y, u);
+        hi[0] = __funnelshift_r(b0.x, b1.x, u); hi[1] = __funnelshift_r(b0.y, b1.y, u);
     }
 };
 template <> struct Tile<4> {
-    static __device__ __forceinline__ void win64(u32 S, u32 u, u32 *lo, u32 *hi) {
-        const u32 a0 = S + 16u * (u >> 5), sh = u & 31u;
-        const uint4 a = lds128(a0), b = lds128(a0 + 16u), c = lds128(a0 + 32u);
-        lo[0] = __funnelshift_r(a.x, b.x, sh); hi[0] = __funnelshift_r(b.x, c.x, sh);
-        lo[1] = __funnelshift_r(a.y, b.y, sh); hi[1] = __funnelshift_r(b.y, c.y, sh);
-        lo[2] = __funnelshift_r(a.z, b.z, sh); hi[2] = __funnelshift_r(b.z, c.z, sh);
-        lo[3] = __funnelshift_r(a.w, b.w, sh); hi[3] = __funnelshift_r(b.w, c.w, sh);
+    static __device__ __forceinline__ void win2(u32 S, u32 u, u32 offb, u32 *lo, u32 *hi) {
+        const u32 a = S + 16u * (u >> 5), b = a + offb;
+        const uint4 a0 = lds128(a), a1 = lds128(a + 16u), b0 = lds128(b), b1 = lds128(b + 16u);
+        lo[0] = __funnelshift_r(a0.x, a1.x, u); lo[1] = __funnelshift_r(a0.y, a1.y, u);
+        lo[2] = __funnelshift_r(a0.z, a1.z, u); lo[3] = __funnelshift_r(a0.w, a1.w, u);
+        hi[0] = __funnelshift_r(b0.x, b1.x, u); hi[1] = __funnelshift_r(b0.y, b1.y, u);
+        hi[2] = __funnelshift_r(b0.z, b1.z, u); hi[3] = __funnelshift_r(b0.w, b1.w, u);
     }
 };
 
-// 64-bit mismatch mask (hi:lo) of a tile window against the base windows
+// 64-bit mismatch mask (hi:lo) of the two half windows against the base windows
 template <int NPP>
-__device__ __forceinline__ u64 mismatch64(u32 S, u32 u, const u32 *blo, const u32 *bhi) {
+__device__ __forceinline__ u64 mismatch2(u32 S, u32 u, u32 offb, const u32 *blo, const u32 *bhi) {
     u32 lo[NPP], hi[NPP];
-    Tile<NPP>::win64(S, u, lo, hi);
+    Tile<NPP>::win2(S, u, offb, lo, hi);
     u32 ml = 0, mh = 0;
 #pragma unroll
     for (int k = 0; k < NPP; ++k) { ml |= lo[k] ^ blo[k]; mh |= hi[k] ^ bhi[k]; }
@@ -484,43 +501,44 @@ struct Item {
     u32 t, s;          // anchor stages, anchor spacing of the epoch
 };
 
-// the stage windows of one lane-word: anchors at tile bit u compared with the
-// windows at u - j dd, j = 1 .. t - 1, in batches of SB loads issued together;
-// a further batch runs only while an anchor of the word is alive.  T > 0 fixes
-// t at compile time (no per-window guard, addresses stepped by dd); T = 0 takes
-// t from the item.  Returns the stages evaluated, base window included.
+// the stage windows of one lane-word: its two 32-anchor halves at tile bits u
+// and u + 8 offb / NPP compared with the windows at u - j dd, j = 1 .. t - 1
+// (each half against its own), in batches of SB issued together.  T > 0 fixes
+// t at compile time: every stage runs (no per-window guard, addresses stepped
+// by dd, no early exit -- some lane of a warp keeps a live anchor to the last
+// stage almost always, so a per-lane exit saves no issue slot).  T = 0 takes t
+// from the item and stops once the word is dead.  Returns the stages
+// evaluated, base window included.
 template <int NPP, int T>
-__device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 dd, u32 t, u64 &alive) {
+__device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 offb, u32 dd, u32 t, u64 &alive) {
     constexpr int SB = NPP == 4 ? CZ_SB4 : (NPP == 2 ? CZ_SB2 : CZ_SB1);
     u32 blo[NPP], bhi[NPP];
-    Tile<NPP>::win64(S, u, blo, bhi);
+    Tile<NPP>::win2(S, u, offb, blo, bhi);
     if constexpr (T > 0) {
-        u32 uj = u, nst = 1;
+        u32 uj = u;
 #pragma unroll
         for (int j0 = 1; j0 < T; j0 += SB) {
-            if (j0 > 1 && !alive) break;
             u64 m[SB];
 #pragma unroll
             for (int k = 0; k < SB; ++k) {
                 if (j0 + k < T) {
                     uj -= dd;
-                    m[k] = mismatch64<NPP>(S, uj, blo, bhi);
+                    m[k] = mismatch2<NPP>(S, uj, offb, blo, bhi);
                 } else {
                     m[k] = 0ull;
                 }
             }
 #pragma unroll
             for (int k = 0; k < SB; ++k) alive &= ~m[k];
-            nst = (u32)(j0 + SB < T ? j0 + SB : T);
         }
-        return nst;
+        return (u32)T;
     } else {
         u32 j = 1;
         while (j < t && alive) {
             u64 m[SB];
 #pragma unroll
             for (int k = 0; k < SB; ++k)
-                m[k] = (j + (u32)k < t) ? mismatch64<NPP>(S, u - (j + (u32)k) * dd, blo, bhi) : 0ull;
+                m[k] = (j + (u32)k < t) ? mismatch2<NPP>(S, u - (j + (u32)k) * dd, offb, blo, bhi) : 0ull;
 #pragma unroll
             for (int k = 0; k < SB; ++k) alive &= ~m[k];
             j += SB;
@@ -529,60 +547,66 @@ __device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 dd, u32 t, u64 &aliv
     }
 }
 
-// the words of row d whose bands start in the item's tile: 64 anchors per
-// lane-word, every stage window read from shared memory.  A lane's rank
-// (anchor k, word w of the band) advances by 32 per pass, stepped
-// incrementally from one division per row.  Survivors are only queued here;
-// when 32 half-words wait for the screen the loop stops at rank `base` and
-// returns false, so the caller screens them with none of this loop's state
-// live and then resumes the row (true: the row is done)
+// the words of row d whose bands start in the item's tile, every stage window
+// read from shared memory.  A band of dd anchors is nw = ceil(dd / 64) pairs of
+// 32-anchor halves: lane-word (k, i) holds halves i and i + nw of band k, so
+// lanes with consecutive ranks read consecutive words.  A lane's rank (k, i)
+// advances by 32 per pass, stepped incrementally from one division per row.
+// Survivors are only queued here; when 32 half-words wait for the screen the
+// loop stops at rank `base` and returns false, so the caller screens them with
+// none of this loop's state live and then resumes the row (true: the row is
+// done)
 template <int NPP, int T>
 __device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u32 d, u32 &base, uint4 *sb,
                                                 WarpQ &q, int lane) {
-    const u32 G = v.G, dd = d / G, t = T > 0 ? (u32)T : it.t;
+    const u32 G = v.G, dd = d >> v.gs, t = T > 0 ? (u32)T : it.t;
     const u32 beta = ((t - 1u) * d + 1u) >> 1;
-    const u32 istart = (beta >= v.c ? beta - v.c + G - 1u : 0u) / G;
+    const u32 istart = (beta >= v.c ? beta - v.c + G - 1u : 0u) >> v.gs;
     if ((i32)istart > v.ihi || istart >= it.T1) return true;
     const u32 step = dd * it.s;
-    const u32 K = ((u32)v.ihi - istart) / step + 1u;
-    const u32 klo = it.T0 > istart ? (it.T0 - istart + step - 1u) / step : 0u;
-    const u32 khi = min(K, (it.T1 - istart + step - 1u) / step);
+    const float rstep = __frcp_rn(__uint2float_rn(step));
+    const u32 K = div_rcp((u32)v.ihi - istart, step, rstep) + 1u;
+    const u32 klo = it.T0 > istart ? div_rcp(it.T0 - istart + step - 1u, step, rstep) : 0u;
+    const u32 khi = min(K, div_rcp(it.T1 - istart + step - 1u, step, rstep));
     if (klo >= khi) return true;
     const u32 nw = (dd + 63u) >> 6;
     const u32 W = (khi - klo) * nw;
     if (base >= W) return true;
-    // rank = base + lane -> (k, w) = (rank / nw, rank % nw); a pass adds
+    // rank = base + lane -> (k, i) = (rank / nw, rank % nw); a pass adds
     // 32 = q32 nw + r32 ranks
     const u32 r0 = base + (u32)lane;
-    u32 k = r0 / nw, w = r0 - k * nw;
-    const u32 q32 = 32u / nw, r32 = 32u - q32 * nw;
-    u32 i0 = istart + (klo + k) * step + 64u * w;          // view index of the lane-word's first anchor
-    const u32 dA = q32 * step + 64u * r32, dB = step - 64u * nw;
+    const float rnw = __frcp_rn(__uint2float_rn(nw));
+    u32 k = div_rcp(r0, nw, rnw), i = r0 - k * nw;
+    const u32 q32 = div_rcp(32u, nw, rnw), r32 = 32u - q32 * nw;
+    u32 i0 = istart + (klo + k) * step + 32u * i;          // view index of the first half's first anchor
+    const u32 dA = q32 * step + 32u * r32, dB = step - 32u * nw;
+    const u32 half = 32u * nw;                              // view distance of the two halves
+    const u32 offb = 4u * (u32)NPP * nw;                    // their byte distance in the tile
     const u32 ubias = v.OFF - it.ubase;
     const u32 S = it.S;
     const i32 ihi = v.ihi;
+    auto mask32 = [](i32 len) { return len >= 32 ? 0xFFFFFFFFu : (len <= 0 ? 0u : ((1u << len) - 1u)); };
     while (base < W) {
         const u32 rank = base + (u32)lane;
         base += 32u;
         u64 alive = 0;
-        const u32 ia = i0;
+        const u32 ia = i0, ib = i0 + half;
         if (rank < W) {
-            // anchors of the word: the band's remaining length, and the view's end
-            i32 len = (i32)(dd - 64u * w);
-            const i32 room = ihi - (i32)ia + 1;
-            if (room < len) len = room;
-            alive = len >= 64 ? ~0ull : (len <= 0 ? 0ull : ((1ull << len) - 1ull));
+            // anchors of each half: the band's remaining length, and the view's end
+            const i32 lena = min((i32)(dd - 32u * i), ihi - (i32)ia + 1);
+            const i32 lenb = min((i32)dd - (i32)(32u * (i + nw)), ihi - (i32)ib + 1);
+            alive = ((u64)mask32(lenb) << 32) | mask32(lena);
         }
-        w += r32;
-        const bool wrap = w >= nw;
-        if (wrap) w -= nw;
+        i += r32;
+        const bool wrap = i >= nw;
+        if (wrap) i -= nw;
         i0 += wrap ? dA + dB : dA;
         if (alive) {
             ++q.words;
-            q.tests += 2u * (u32)NPP * run_stages<NPP, T>(S, ia + ubias, dd, t, alive);
+            q.tests += 2u * (u32)NPP * run_stages<NPP, T>(S, ia + ubias, offb, dd, t, alive);
         }
         queue_append(sb, q, ia, (u32)alive, d, t, lane);
-        queue_append(sb, q, ia + 32u, (u32)(alive >> 32), d, t, lane);
+        queue_append(sb, q, ib, (u32)(alive >> 32), d, t, lane);
         if (q.nscr >= 32u) return base >= W;
     }
     return true;
@@ -751,10 +775,10 @@ __device__ __noinline__ void load_profile(const SparseArgs &a, u32 gprof, ProfCt
     c.NW = PR.nwords; c.NW2 = PR.nwords2; c.OFF = 32u * PR.K0 + 31u; c.ex = (PR.p - 1u) / PD.r;
     c.M = Mont{PR.p, PR.ninv, PR.one, PR.r2};
     c.P = a.planes + PD.plane_off;
-    c.base = View{c.P, c.OFF, -(i32)PR.B, (i32)PR.B, 1u, 0u};
+    c.base = View{c.P, c.OFF, -(i32)PR.B, (i32)PR.B, 1u, 0u, 0u};
     // odd view: n = 2i + 1 in [-B, B]  <=>  i in [ceil((-B-1)/2), floor((B-1)/2)]
     c.odd = View{c.P + (size_t)PR.nwords * PD.npp, 32u * PR.K2, -(i32)((PR.B + 1u) / 2u), (i32)((PR.B - 1u) / 2u),
-                 2u, 1u};
+                 2u, 1u, 1u};
     for (int j = 0; j < 9; ++j) c.om[j] = PD.omega[j];
     c.seed = *(volatile u32 *)&a.state[gprof].seed;
     c.qspec = PD.qspec;

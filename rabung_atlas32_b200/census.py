@@ -36,7 +36,7 @@ class Tuning:
     screen: int = 1
     sparse_blocks: int = 0
     use_graph: int = 1
-    cta_per_profile: int = 2
+    cta_per_profile: int = 1
     epoch_rows: int = 1024
     speculate: int = 1
     spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 10, 0, 5, 10)

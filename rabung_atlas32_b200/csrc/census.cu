@@ -32,7 +32,7 @@ int cz_default_config(cz_config *c) {
     c->screen = 1;
     c->sparse_blocks = 0;
     c->use_graph = 1;
-    c->cta_per_profile = 2;
+    c->cta_per_profile = 1;
     c->epoch_rows = EPOCH_ROWS_DEFAULT;
     c->speculate = 1;
     c->plane_budget_mb = 24u * 1024u;

@@ -507,17 +507,21 @@ struct Item {
 // t at compile time: every stage runs (no per-window guard, addresses stepped
 // by dd, no early exit -- some lane of a warp keeps a live anchor to the last
 // stage almost always, so a per-lane exit saves no issue slot).  T = 0 takes t
-// from the item and stops once the word is dead.  Returns the stages
-// evaluated, base window included.
+// from the item and stops once the word is dead.  Returns the stages a word
+// needs, base window included: those of the batches begun while it was alive,
+// the same count in both forms.
 template <int NPP, int T>
 __device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 offb, u32 dd, u32 t, u64 &alive) {
     constexpr int SB = NPP == 4 ? CZ_SB4 : (NPP == 2 ? CZ_SB2 : CZ_SB1);
     u32 blo[NPP], bhi[NPP];
     Tile<NPP>::win2(S, u, offb, blo, bhi);
     if constexpr (T > 0) {
-        u32 uj = u;
+        // nst: the stages the generic loop would evaluate (batches begun while
+        // the word was alive), the algorithmic work counted for the roofline
+        u32 uj = u, nst = 1;
 #pragma unroll
         for (int j0 = 1; j0 < T; j0 += SB) {
+            if (alive) nst = (u32)(j0 + SB < T ? j0 + SB : T);
             u64 m[SB];
 #pragma unroll
             for (int k = 0; k < SB; ++k) {
@@ -531,7 +535,7 @@ __device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 offb, u32 dd, u32 t,
 #pragma unroll
             for (int k = 0; k < SB; ++k) alive &= ~m[k];
         }
-        return (u32)T;
+        return nst;
     } else {
         u32 j = 1;
         while (j < t && alive) {

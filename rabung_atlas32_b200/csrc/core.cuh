@@ -145,7 +145,10 @@ bool ensure(CZ_HANDLE *h, Buf &b, size_t bytes) {
 template <class T> T *P(Buf &b) { return reinterpret_cast<T *>(b.p); }
 
 bool build_static_tables(CZ_HANDLE *h) {
-    // primes below CHAIN_LIMIT and the smallest-prime-factor chain
+    // primes below CHAIN_LIMIT and the prime-power chain: chain[n] =
+    // (index of q = spf(n) | e << 24, n / q^e) with q^e the full power of q in
+    // n, so a walk takes one step per distinct prime factor (at most 7 below
+    // 2^20), not one per factor
     std::vector<u32> spf(CHAIN_LIMIT, 0);
     std::vector<u32> primes;
     for (u32 i = 2; i < CHAIN_LIMIT; ++i) {
@@ -162,7 +165,12 @@ bool build_static_tables(CZ_HANDLE *h) {
     std::vector<uint2> chain(CHAIN_LIMIT);
     chain[0] = make_uint2(0, 0);
     chain[1] = make_uint2(0, 1);
-    for (u32 n = 2; n < CHAIN_LIMIT; ++n) chain[n] = make_uint2(index[spf[n]], n / spf[n]);
+    for (u32 n = 2; n < CHAIN_LIMIT; ++n) {
+        const u32 q = spf[n];
+        u32 m = n, e = 0;
+        while (m % q == 0) { m /= q; ++e; }
+        chain[n] = make_uint2(index[q] | (e << 24), m);     // index < 2^17, e <= 20
+    }
     h->n_small = (u32)primes.size();
     if (!ck(h, cudaMalloc(&h->d_small, primes.size() * 4), "cudaMalloc small")) return false;
     if (!ck(h, cudaMalloc(&h->d_chain, chain.size() * sizeof(uint2)), "cudaMalloc chain")) return false;

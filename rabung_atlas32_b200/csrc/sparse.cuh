@@ -58,6 +58,21 @@ namespace CZ_NS {
 #ifndef CZ_SB1                       // anchor stages whose loads issue together, by stored planes
 #define CZ_SB1 5                     // r = 2 runs t - 1 = 10 stages: two batches of 5
 #endif
+#ifndef CZ_TS1                       // anchor stage counts whose stage loops are compiled for a
+#define CZ_TS1 11                    // fixed t, by stored planes (the measured anchor_t per order:
+#endif                               // r = 2: 11; r = 3, 4: 7, 6; r = 5: 5; r = 6..9: 4)
+#ifndef CZ_TS2A
+#define CZ_TS2A 7
+#endif
+#ifndef CZ_TS2B
+#define CZ_TS2B 6
+#endif
+#ifndef CZ_TS4A
+#define CZ_TS4A 5
+#endif
+#ifndef CZ_TS4B
+#define CZ_TS4B 4
+#endif
 #ifndef CZ_SB2
 #define CZ_SB2 2
 #endif
@@ -630,19 +645,19 @@ __device__ __forceinline__ void filter_item(const ProfCtx &c, const Item &it, co
         const View &v = it.view ? c.odd : c.base;
         u32 base = 0;
         for (;;) {
-            // the anchor stage counts of the default tuning run with t fixed at compile time
+            // the anchor stage counts CZ_TS* (the default tuning's) run with t fixed at compile time
             bool done;
             if constexpr (NPP == 1) {
-                done = it.t == 11u ? filter_row_tile<1, 11>(v, it, d, base, sb, q, lane)
-                                   : filter_row_tile<1, 0>(v, it, d, base, sb, q, lane);
+                done = it.t == CZ_TS1 ? filter_row_tile<1, CZ_TS1>(v, it, d, base, sb, q, lane)
+                                      : filter_row_tile<1, 0>(v, it, d, base, sb, q, lane);
             } else if constexpr (NPP == 2) {
-                done = it.t == 7u ? filter_row_tile<2, 7>(v, it, d, base, sb, q, lane)
-                     : it.t == 6u ? filter_row_tile<2, 6>(v, it, d, base, sb, q, lane)
-                                  : filter_row_tile<2, 0>(v, it, d, base, sb, q, lane);
+                done = it.t == CZ_TS2A ? filter_row_tile<2, CZ_TS2A>(v, it, d, base, sb, q, lane)
+                     : it.t == CZ_TS2B ? filter_row_tile<2, CZ_TS2B>(v, it, d, base, sb, q, lane)
+                                       : filter_row_tile<2, 0>(v, it, d, base, sb, q, lane);
             } else {
-                done = it.t == 5u ? filter_row_tile<4, 5>(v, it, d, base, sb, q, lane)
-                     : it.t == 4u ? filter_row_tile<4, 4>(v, it, d, base, sb, q, lane)
-                                  : filter_row_tile<4, 0>(v, it, d, base, sb, q, lane);
+                done = it.t == CZ_TS4A ? filter_row_tile<4, CZ_TS4A>(v, it, d, base, sb, q, lane)
+                     : it.t == CZ_TS4B ? filter_row_tile<4, CZ_TS4B>(v, it, d, base, sb, q, lane)
+                                       : filter_row_tile<4, 0>(v, it, d, base, sb, q, lane);
             }
             while (q.nscr >= 32u) screen_batch<NPP>(c, sb, cb, q, 32u, screen, st, lane);
             if (done) break;

@@ -19,8 +19,10 @@
 // B200 design:
 //  * labels are computed only for primes q in the table (one Montgomery power
 //    each, kept in shared memory); every other n takes its label additively
-//    through a smallest-prime-factor chain n -> n / spf(n) (the colour is a
-//    character), so a table of ~10^6 entries costs ~6e4 powers, not 10^6;
+//    through a prime-power chain n -> n / q^e, q = spf(n) (the colour is a
+//    character: label(n) = sum of e label(q)), so a table of ~10^6 entries
+//    costs ~6e4 powers, not 10^6, and a walk takes one step per distinct
+//    prime factor;
 //  * each warp stages 32 consecutive labels per step in shared memory, then
 //    emits plane words profile by profile with one ballot per plane bit: the
 //    negative half of the base view is one __brev'd ballot (aligned by the
@@ -52,7 +54,7 @@ struct TableArgs {
     u32 nsparse;
     const u32 *small_primes;     // all primes below chain_limit, ascending
     u32 n_small;
-    const uint2 *chain;          // chain[n] = (index of spf(n) in small_primes, n / spf(n))
+    const uint2 *chain;          // chain[n] = (index of q = spf(n) in small_primes | e << 24, n / q^e)
     u32 chain_limit;
 };
 
@@ -165,7 +167,7 @@ table_kernel(TableArgs a) {
                     for (u32 i = 0; i <= TABLE_SUB; ++i) {
                         if (v[i] > 1u) {
                             const uint2 c = a.chain[v[i]];
-                            l[i] += plab[c.x];
+                            l[i] += (c.x >> 24) * plab[c.x & 0xFFFFFFu];   // e label(q): the sum stays <= 20 (m - 1)
                             v[i] = c.y;
                             any = true;
                         }

@@ -19,7 +19,7 @@
 //    b are enumerated, on the odd-numerator view of the table (the reference's
 //    G = 2 wheel, PBV/src/wheel_filter.hpp:14-46).
 //  * Filter (PBV/src/wheel_filter.hpp:52-91): a candidate anchor survives while
-//    every offset b - jd (j < t) agrees with b on every colour plane; here 64
+//    every offset b - jd (j < t) agrees with b on every colour plane; here 96
 //    anchors per lane-word, their stages in batches whose loads issue together.
 //  * Bilateral screen (B1/src/two_cuts.hpp:27-74): reject only when known
 //    mismatches on both sides bound the run below the verified maximum;
@@ -33,8 +33,8 @@
 //    run (or its reflection) is completed.
 //
 // B200 design: one persistent kernel over all profiles of a call, handed out
-// longest first; a group of CTAs (2 for large calls, up to 64 when a call has
-// few profiles) shares one (p, r) profile.  A profile's rows d are cut into
+// longest first; a group of CTAs (cta_per_profile, 1 by default, for large
+// calls; up to 64 when a call has few profiles) shares one (p, r) profile.  A profile's rows d are cut into
 // epochs of consecutive d, each run with one threshold q -- the verified
 // maximum (or the speculative threshold) when the epoch's first work item is
 // claimed -- so the threshold rises between epochs and every row keeps one q.
@@ -45,10 +45,12 @@
 // by one bulk asynchronous copy (cp.async.bulk, completed on an mbarrier), so
 // every anchor-stage window is a shared-memory load instead of an L1/L2 one.
 // Warps claim the item's rows from a shared counter; lanes take consecutive
-// 64-anchor words of a row; a window is cut from three plane words by funnel
-// shifts; words that survive are queued per warp (across rows and items of a
-// profile) and screened 32 at a time, one per lane, against the planes in
-// global memory, and the screened candidates are completed 32 at a time.
+// 96-anchor lane-words of a row (three 32-bit words, so a warp's loads are
+// three words apart and conflict-free); a stage's three windows are cut from
+// four plane words by funnel shifts; words that survive are queued per warp
+// (across rows and items of a profile) and screened 32 at a time, one per
+// lane, against the planes in global memory, and the screened candidates are
+// completed 32 at a time.
 #pragma once
 #include "labels.cuh"
 #include "finalize.cuh"
@@ -95,7 +97,7 @@ constexpr u32 MBAR_SPIN_LIMIT = 1u << 22;   // bounded wait on a tile copy
 #endif
 constexpr int SPARSE_WARPS = CZ_SPARSE_WARPS;
 constexpr int CAND_CAP = 64;          // per-warp buffer of candidates awaiting completion
-constexpr int SCR_CAP = 96;           // per-warp buffer of words awaiting the screen (< 32 + two half-words of 32)
+constexpr int SCR_CAP = 128;          // per-warp buffer of words awaiting the screen (< 32 + three words of 32)
 constexpr u32 RUN_CAP = 4096;         // longest run a completion may walk
 
 struct Tuning {
@@ -124,6 +126,11 @@ struct SparseArgs {
 };
 
 struct Cand { u32 b, d; };
+
+// a word awaiting the screen: view index of its bit 0, its surviving anchors,
+// and its row d and stages t packed as d << 8 | t (d <= D <= 2^20 by the
+// cover, t <= Q <= 255 by the configuration)
+struct QEnt { u32 i0, alive, dt; };
 
 // preferred anchor length: least t with r^(t-1) >= 2^(5+bits), i.e. a word of
 // 32 random anchors keeps on average <= 2^-bits survivors
@@ -362,16 +369,16 @@ __device__ __forceinline__ u32 threshold(const ProfCtx &c, ProfState *st) {
 // (d, t) -- and queue the surviving candidates for completion; the queue is
 // carried across rows, so batches stay full
 template <int NPP>
-__device__ __forceinline__ void screen_batch(const ProfCtx &c, uint4 *sb, Cand *cb, WarpQ &q, u32 count,
+__device__ __forceinline__ void screen_batch(const ProfCtx &c, QEnt *sb, Cand *cb, WarpQ &q, u32 count,
                                              bool screen, ProfState *st, int lane) {
     u32 keep = 0, i0 = 0, d = 0, vc = 0, vg = 1;
     const u32 thr = threshold(c, st);
     if ((u32)lane < count) {
-        const uint4 e = sb[lane];
-        i0 = e.x;
-        keep = e.y;
-        d = e.z;
-        const u32 t = e.w;
+        const QEnt e = sb[lane];
+        i0 = e.i0;
+        keep = e.alive;
+        d = e.dt >> 8;
+        const u32 t = e.dt & 0xFFu;
         const View &v = (d & 1u) ? c.base : c.odd;
         vc = v.c;
         vg = v.G;
@@ -400,14 +407,14 @@ __device__ __forceinline__ void screen_batch(const ProfCtx &c, uint4 *sb, Cand *
 }
 
 
-// queue one 32-bit half-word per lane for the batched screen; the caller runs
+// queue one 32-bit word per lane for the batched screen; the caller runs
 // the screen once 32 are waiting (the buffer holds SCR_CAP)
-__device__ __forceinline__ void queue_append(uint4 *sb, WarpQ &q, u32 i0, u32 alive, u32 d, u32 t, int lane) {
+__device__ __forceinline__ void queue_append(QEnt *sb, WarpQ &q, u32 i0, u32 alive, u32 d, u32 t, int lane) {
     const bool has = alive != 0u;
     const u32 bal = __ballot_sync(0xFFFFFFFFu, has);
     if (!bal) return;
     const u32 pos = __popc(bal & ((1u << lane) - 1u));
-    if (has) sb[q.nscr + pos] = make_uint4(i0, alive, d, t);
+    if (has) sb[q.nscr + pos] = QEnt{i0, alive, (d << 8) | t};
     q.nscr += __popc(bal);
     __syncwarp();
 }
@@ -461,49 +468,58 @@ __device__ __forceinline__ void bulk_load(u32 dst, const void *src, u32 bytes, u
                  :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
-// two 32-bit windows of the NPP interleaved planes of a tile at shared byte
-// address S (word w of plane k at S + 4 (w NPP + k)): lo = bits [u, u+32) and
-// hi = bits [u + 32 nb, u + 32 nb + 32), where offb = 4 NPP nb is the byte
-// distance of the two halves.  Both halves share the shift u mod 32; each
-// reads two consecutive words, so lanes holding consecutive words of a band
-// read consecutive shared addresses (no bank conflicts)
+// three consecutive 32-bit windows of the NPP interleaved planes of a tile at
+// shared byte address S (word w of plane k at S + 4 (w NPP + k)): o[c] = bits
+// [u + 32 c, u + 32 c + 32), from the four words that hold bits [u, u + 96).
+// Lanes holding consecutive lane-words of a band read words three apart: every
+// load of a warp is conflict-free at each width (3 l mod 32, mod 16 and mod 8
+// are distinct over the lanes that share a wavefront), and the four loads of
+// a window give 96 anchors.
 template <int NPP> struct Tile;
 template <> struct Tile<1> {
-    static __device__ __forceinline__ void win2(u32 S, u32 u, u32 offb, u32 *lo, u32 *hi) {
-        const u32 a = S + 4u * (u >> 5), b = a + offb;
-        const u32 a0 = lds32(a), a1 = lds32(a + 4u), b0 = lds32(b), b1 = lds32(b + 4u);
-        lo[0] = __funnelshift_r(a0, a1, u);
-        hi[0] = __funnelshift_r(b0, b1, u);
+    static __device__ __forceinline__ void win3(u32 S, u32 u, u32 (*o)[1]) {
+        const u32 a = S + 4u * (u >> 5);
+        const u32 p0 = lds32(a), p1 = lds32(a + 4u), p2 = lds32(a + 8u), p3 = lds32(a + 12u);
+        o[0][0] = __funnelshift_r(p0, p1, u);
+        o[1][0] = __funnelshift_r(p1, p2, u);
+        o[2][0] = __funnelshift_r(p2, p3, u);
     }
 };
 template <> struct Tile<2> {
-    static __device__ __forceinline__ void win2(u32 S, u32 u, u32 offb, u32 *lo, u32 *hi) {
-        const u32 a = S + 8u * (u >> 5), b = a + offb;
-        const uint2 a0 = lds64(a), a1 = lds64(a + 8u), b0 = lds64(b), b1 = lds64(b + 8u);
-        lo[0] = __funnelshift_r(a0.x, a1.x, u); lo[1] = __funnelshift_r(a0.y, a1.y, u);
-        hi[0] = __funnelshift_r(b0.x, b1.x, u); hi[1] = __funnelshift_r(b0.y, b1.y, u);
+    static __device__ __forceinline__ void win3(u32 S, u32 u, u32 (*o)[2]) {
+        const u32 a = S + 8u * (u >> 5);
+        const uint2 p0 = lds64(a), p1 = lds64(a + 8u), p2 = lds64(a + 16u), p3 = lds64(a + 24u);
+        o[0][0] = __funnelshift_r(p0.x, p1.x, u); o[0][1] = __funnelshift_r(p0.y, p1.y, u);
+        o[1][0] = __funnelshift_r(p1.x, p2.x, u); o[1][1] = __funnelshift_r(p1.y, p2.y, u);
+        o[2][0] = __funnelshift_r(p2.x, p3.x, u); o[2][1] = __funnelshift_r(p2.y, p3.y, u);
     }
 };
 template <> struct Tile<4> {
-    static __device__ __forceinline__ void win2(u32 S, u32 u, u32 offb, u32 *lo, u32 *hi) {
-        const u32 a = S + 16u * (u >> 5), b = a + offb;
-        const uint4 a0 = lds128(a), a1 = lds128(a + 16u), b0 = lds128(b), b1 = lds128(b + 16u);
-        lo[0] = __funnelshift_r(a0.x, a1.x, u); lo[1] = __funnelshift_r(a0.y, a1.y, u);
-        lo[2] = __funnelshift_r(a0.z, a1.z, u); lo[3] = __funnelshift_r(a0.w, a1.w, u);
-        hi[0] = __funnelshift_r(b0.x, b1.x, u); hi[1] = __funnelshift_r(b0.y, b1.y, u);
-        hi[2] = __funnelshift_r(b0.z, b1.z, u); hi[3] = __funnelshift_r(b0.w, b1.w, u);
+    static __device__ __forceinline__ void win3(u32 S, u32 u, u32 (*o)[4]) {
+        const u32 a = S + 16u * (u >> 5);
+        const uint4 p0 = lds128(a), p1 = lds128(a + 16u), p2 = lds128(a + 32u), p3 = lds128(a + 48u);
+        o[0][0] = __funnelshift_r(p0.x, p1.x, u); o[0][1] = __funnelshift_r(p0.y, p1.y, u);
+        o[0][2] = __funnelshift_r(p0.z, p1.z, u); o[0][3] = __funnelshift_r(p0.w, p1.w, u);
+        o[1][0] = __funnelshift_r(p1.x, p2.x, u); o[1][1] = __funnelshift_r(p1.y, p2.y, u);
+        o[1][2] = __funnelshift_r(p1.z, p2.z, u); o[1][3] = __funnelshift_r(p1.w, p2.w, u);
+        o[2][0] = __funnelshift_r(p2.x, p3.x, u); o[2][1] = __funnelshift_r(p2.y, p3.y, u);
+        o[2][2] = __funnelshift_r(p2.z, p3.z, u); o[2][3] = __funnelshift_r(p2.w, p3.w, u);
     }
 };
 
-// 64-bit mismatch mask (hi:lo) of the two half windows against the base windows
+// kill the anchors of the three words whose stage window at u differs from
+// their base windows in any plane
 template <int NPP>
-__device__ __forceinline__ u64 mismatch2(u32 S, u32 u, u32 offb, const u32 *blo, const u32 *bhi) {
-    u32 lo[NPP], hi[NPP];
-    Tile<NPP>::win2(S, u, offb, lo, hi);
-    u32 ml = 0, mh = 0;
+__device__ __forceinline__ void mismatch3(u32 S, u32 u, const u32 (*b)[NPP], u32 *alive) {
+    u32 w[3][NPP];
+    Tile<NPP>::win3(S, u, w);
 #pragma unroll
-    for (int k = 0; k < NPP; ++k) { ml |= lo[k] ^ blo[k]; mh |= hi[k] ^ bhi[k]; }
-    return ((u64)mh << 32) | ml;
+    for (int c = 0; c < 3; ++c) {
+        u32 m = 0;
+#pragma unroll
+        for (int k = 0; k < NPP; ++k) m |= w[c][k] ^ b[c][k];
+        alive[c] &= ~m;
+    }
 }
 
 // one work item as staged in shared memory
@@ -516,50 +532,39 @@ struct Item {
     u32 t, s;          // anchor stages, anchor spacing of the epoch
 };
 
-// the stage windows of one lane-word: its two 32-anchor halves at tile bits u
-// and u + 8 offb / NPP compared with the windows at u - j dd, j = 1 .. t - 1
-// (each half against its own), in batches of SB issued together.  T > 0 fixes
-// t at compile time: every stage runs (no per-window guard, addresses stepped
-// by dd, no early exit -- some lane of a warp keeps a live anchor to the last
-// stage almost always, so a per-lane exit saves no issue slot).  T = 0 takes t
-// from the item and stops once the word is dead.  Returns the stages a word
-// needs, base window included: those of the batches begun while it was alive,
-// the same count in both forms.
+// the stage windows of one lane-word: its 96 anchors at tile bits [u, u + 96)
+// compared with the windows at u - j dd, j = 1 .. t - 1, in batches of SB
+// issued together.  T > 0 fixes t at compile time: every stage runs (no
+// per-window guard, addresses stepped by dd, no early exit -- some lane of a
+// warp keeps a live anchor to the last stage almost always, so a per-lane exit
+// saves no issue slot).  T = 0 takes t from the item and stops once the word
+// is dead.  Returns the stages a word needs, base window included: those of
+// the batches begun while it was alive, the same count in both forms.
 template <int NPP, int T>
-__device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 offb, u32 dd, u32 t, u64 &alive) {
+__device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 dd, u32 t, u32 *alive) {
     constexpr int SB = NPP == 4 ? CZ_SB4 : (NPP == 2 ? CZ_SB2 : CZ_SB1);
-    u32 blo[NPP], bhi[NPP];
-    Tile<NPP>::win2(S, u, offb, blo, bhi);
+    u32 b[3][NPP];
+    Tile<NPP>::win3(S, u, b);
     if constexpr (T > 0) {
-        // nst: the stages the generic loop would evaluate (batches begun while
-        // the word was alive), the algorithmic work counted for the roofline
         u32 uj = u, nst = 1;
 #pragma unroll
         for (int j0 = 1; j0 < T; j0 += SB) {
-            if (alive) nst = (u32)(j0 + SB < T ? j0 + SB : T);
-            u64 m[SB];
+            if (alive[0] | alive[1] | alive[2]) nst = (u32)(j0 + SB < T ? j0 + SB : T);
 #pragma unroll
             for (int k = 0; k < SB; ++k) {
                 if (j0 + k < T) {
                     uj -= dd;
-                    m[k] = mismatch2<NPP>(S, uj, offb, blo, bhi);
-                } else {
-                    m[k] = 0ull;
+                    mismatch3<NPP>(S, uj, b, alive);
                 }
             }
-#pragma unroll
-            for (int k = 0; k < SB; ++k) alive &= ~m[k];
         }
         return nst;
     } else {
         u32 j = 1;
-        while (j < t && alive) {
-            u64 m[SB];
+        while (j < t && (alive[0] | alive[1] | alive[2])) {
 #pragma unroll
             for (int k = 0; k < SB; ++k)
-                m[k] = (j + (u32)k < t) ? mismatch2<NPP>(S, u - (j + (u32)k) * dd, offb, blo, bhi) : 0ull;
-#pragma unroll
-            for (int k = 0; k < SB; ++k) alive &= ~m[k];
+                if (j + (u32)k < t) mismatch3<NPP>(S, u - (j + (u32)k) * dd, b, alive);
             j += SB;
         }
         return min(j, t);
@@ -567,16 +572,16 @@ __device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 offb, u32 dd, u32 t,
 }
 
 // the words of row d whose bands start in the item's tile, every stage window
-// read from shared memory.  A band of dd anchors is nw = ceil(dd / 64) pairs of
-// 32-anchor halves: lane-word (k, i) holds halves i and i + nw of band k, so
-// lanes with consecutive ranks read consecutive words.  A lane's rank (k, i)
+// read from shared memory.  A band of dd anchors is nw = ceil(dd / 96)
+// lane-words of 96 consecutive anchors (three 32-bit words); lanes with
+// consecutive ranks hold consecutive lane-words.  A lane's rank (k, w)
 // advances by 32 per pass, stepped incrementally from one division per row.
-// Survivors are only queued here; when 32 half-words wait for the screen the
+// Survivors are only queued here; when 32 words wait for the screen the
 // loop stops at rank `base` and returns false, so the caller screens them with
 // none of this loop's state live and then resumes the row (true: the row is
 // done)
 template <int NPP, int T>
-__device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u32 d, u32 &base, uint4 *sb,
+__device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u32 d, u32 &base, QEnt *sb,
                                                 WarpQ &q, int lane) {
     const u32 G = v.G, dd = d >> v.gs, t = T > 0 ? (u32)T : it.t;
     const u32 beta = ((t - 1u) * d + 1u) >> 1;
@@ -588,7 +593,7 @@ __device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u
     const u32 klo = it.T0 > istart ? div_rcp(it.T0 - istart + step - 1u, step, rstep) : 0u;
     const u32 khi = min(K, div_rcp(it.T1 - istart + step - 1u, step, rstep));
     if (klo >= khi) return true;
-    const u32 nw = (dd + 63u) >> 6;
+    const u32 nw = div_rcp(dd + 95u, 96u, 1.0f / 96.0f);   // lane-words per band
     const u32 W = (khi - klo) * nw;
     if (base >= W) return true;
     // rank = base + lane -> (k, i) = (rank / nw, rank % nw); a pass adds
@@ -597,10 +602,8 @@ __device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u
     const float rnw = __frcp_rn(__uint2float_rn(nw));
     u32 k = div_rcp(r0, nw, rnw), i = r0 - k * nw;
     const u32 q32 = div_rcp(32u, nw, rnw), r32 = 32u - q32 * nw;
-    u32 i0 = istart + (klo + k) * step + 32u * i;          // view index of the first half's first anchor
-    const u32 dA = q32 * step + 32u * r32, dB = step - 32u * nw;
-    const u32 half = 32u * nw;                              // view distance of the two halves
-    const u32 offb = 4u * (u32)NPP * nw;                    // their byte distance in the tile
+    u32 i0 = istart + (klo + k) * step + 96u * i;          // view index of the lane-word's first anchor
+    const u32 dA = q32 * step + 96u * r32, dB = step - 96u * nw;
     const u32 ubias = v.OFF - it.ubase;
     const u32 S = it.S;
     const i32 ihi = v.ihi;
@@ -608,24 +611,29 @@ __device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u
     while (base < W) {
         const u32 rank = base + (u32)lane;
         base += 32u;
-        u64 alive = 0;
-        const u32 ia = i0, ib = i0 + half;
+        u32 alive[3] = {0u, 0u, 0u};
+        const u32 ia = i0;
         if (rank < W) {
-            // anchors of each half: the band's remaining length, and the view's end
-            const i32 lena = min((i32)(dd - 32u * i), ihi - (i32)ia + 1);
-            const i32 lenb = min((i32)dd - (i32)(32u * (i + nw)), ihi - (i32)ib + 1);
-            alive = ((u64)mask32(lenb) << 32) | mask32(lena);
+            // anchors of the word: the band's remaining length, and the view's end
+            const i32 len = min((i32)(dd - 96u * i), ihi - (i32)ia + 1);
+            alive[0] = mask32(len);
+            alive[1] = mask32(len - 32);
+            alive[2] = mask32(len - 64);
         }
         i += r32;
         const bool wrap = i >= nw;
         if (wrap) i -= nw;
         i0 += wrap ? dA + dB : dA;
-        if (alive) {
+        if (alive[0]) {
+            // algorithmic tests: stage x plane comparisons of the 32-bit words
+            // that hold anchors of the band (one to three per lane-word)
+            const u32 live = 1u + (alive[1] != 0u) + (alive[2] != 0u);
             ++q.words;
-            q.tests += 2u * (u32)NPP * run_stages<NPP, T>(S, ia + ubias, offb, dd, t, alive);
+            q.tests += live * (u32)NPP * run_stages<NPP, T>(S, ia + ubias, dd, t, alive);
         }
-        queue_append(sb, q, ia, (u32)alive, d, t, lane);
-        queue_append(sb, q, ib, (u32)(alive >> 32), d, t, lane);
+        queue_append(sb, q, ia, alive[0], d, t, lane);
+        queue_append(sb, q, ia + 32u, alive[1], d, t, lane);
+        queue_append(sb, q, ia + 64u, alive[2], d, t, lane);
         if (q.nscr >= 32u) return base >= W;
     }
     return true;
@@ -634,7 +642,7 @@ __device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u
 // the rows of the staged item, claimed one per warp from a shared counter
 template <int NPP>
 __device__ __forceinline__ void filter_item(const ProfCtx &c, const Item &it, const SparseArgs &a, u32 *row_ctr,
-                                            uint4 *sb, Cand *cb, WarpQ &q, ProfState *st, int lane) {
+                                            QEnt *sb, Cand *cb, WarpQ &q, ProfState *st, int lane) {
     const bool screen = a.tune.screen != 0u;
     for (;;) {
         u32 r = 0;
@@ -814,7 +822,7 @@ sparse_kernel(SparseArgs a) {
     __shared__ unsigned long long s_mbar;
     __shared__ u32 s_item, s_err, s_row, s_has, s_phase;
     __shared__ Cand cbuf[SPARSE_WARPS][CAND_CAP];      // candidates awaiting completion
-    __shared__ uint4 sbuf[SPARSE_WARPS][SCR_CAP];      // (index, alive, d, t) words awaiting the screen
+    __shared__ QEnt sbuf[SPARSE_WARPS][SCR_CAP];       // words awaiting the screen
     __shared__ ProfCtx s_ctx;
     __shared__ Item s_it;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -840,7 +848,7 @@ sparse_kernel(SparseArgs a) {
         const ProfCtx &c = s_ctx;
         ProfState *st = a.state + a.prof_list[pitem];
         WarpQ q{0, 0, 0, 0, 0, 0, 0};
-        uint4 *sb = sbuf[warp];
+        QEnt *sb = sbuf[warp];
         Cand *cb = cbuf[warp];
         for (;;) {
             if (threadIdx.x == 0) {

@@ -42,7 +42,7 @@ class Tuning:
     spec_margin10: tuple = (0, 0, 30, 20, 15, 15, 10, 0, 5, 10)
     plane_budget_mb: int = 24 * 1024
     dense_steps: int = 256
-    anchor_t: tuple = (0, 0, 11, 7, 6, 5, 4, 4, 4, 4)
+    anchor_t: tuple = (0, 0, 11, 7, 6, 5, 5, 5, 5, 5)
 
 
 def _as_u32_array(values):

@@ -39,7 +39,7 @@ int cz_default_config(cz_config *c) {
     c->dense_steps = DENSE_STEPS;
     const u32 sm[10] = {0, 0, 30, 20, 15, 15, 10, 0, 5, 10};   // measured per order
     for (int r = 0; r < 10; ++r) c->spec_margin10[r] = sm[r];
-    const u32 at[10] = {0, 0, 11, 7, 6, 5, 4, 4, 4, 4};   // measured per order on a top block
+    const u32 at[10] = {0, 0, 11, 7, 6, 5, 5, 5, 5, 5};   // measured per order on a top block
     for (int r = 0; r < 10; ++r) c->anchor_t[r] = at[r];
     return CZ_OK;
 }

@@ -62,7 +62,7 @@ namespace CZ_NS {
 #endif
 #ifndef CZ_TS1                       // anchor stage counts whose stage loops are compiled for a
 #define CZ_TS1 11                    // fixed t, by stored planes (the measured anchor_t per order:
-#endif                               // r = 2: 11; r = 3, 4: 7, 6; r = 5: 5; r = 6..9: 4)
+#endif                               // r = 2: 11; r = 3, 4: 7, 6; r = 5..9: 5; 4 the earlier r = 6..9)
 #ifndef CZ_TS2A
 #define CZ_TS2A 7
 #endif

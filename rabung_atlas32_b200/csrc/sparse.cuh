@@ -58,8 +58,8 @@
 namespace CZ_NS {
 
 #ifndef CZ_SB1                       // anchor stages whose loads issue together, by stored planes
-#define CZ_SB1 5                     // r = 2 runs t - 1 = 10 stages: two batches of 5
-#endif
+#define CZ_SB1 5                     // (measured on 96-anchor words: r = 2 runs 10 stages as 5 + 5;
+#endif                               // 2 planes 3 + 3, 3 + 2; 4 planes 2 + 2)
 #ifndef CZ_TS1                       // anchor stage counts whose stage loops are compiled for a
 #define CZ_TS1 11                    // fixed t, by stored planes (the measured anchor_t per order:
 #endif                               // r = 2: 11; r = 3, 4: 7, 6; r = 5..9: 5; 4 the earlier r = 6..9)
@@ -76,10 +76,10 @@ namespace CZ_NS {
 #define CZ_TS4B 4
 #endif
 #ifndef CZ_SB2
-#define CZ_SB2 2
+#define CZ_SB2 3
 #endif
 #ifndef CZ_SB4
-#define CZ_SB4 1
+#define CZ_SB4 2
 #endif
 #ifndef CZ_SPARSE_MINB                // resident filter CTAs per SM (register budget)
 #define CZ_SPARSE_MINB 2

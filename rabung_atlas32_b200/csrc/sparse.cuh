@@ -582,7 +582,7 @@ __device__ __forceinline__ u32 run_stages(u32 S, u32 u, u32 dd, u32 t, u32 *aliv
 // done)
 template <int NPP, int T>
 __device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u32 d, u32 &base, QEnt *sb,
-                                                WarpQ &q, int lane) {
+                                                WarpQ &q, int lane, u32 np) {
     const u32 G = v.G, dd = d >> v.gs, t = T > 0 ? (u32)T : it.t;
     const u32 beta = ((t - 1u) * d + 1u) >> 1;
     const u32 istart = (beta >= v.c ? beta - v.c + G - 1u : 0u) >> v.gs;
@@ -626,10 +626,12 @@ __device__ __forceinline__ bool filter_row_tile(const View &v, const Item &it, u
         i0 += wrap ? dA + dB : dA;
         if (alive[0]) {
             // algorithmic tests: stage x plane comparisons of the 32-bit words
-            // that hold anchors of the band (one to three per lane-word)
+            // that hold anchors of the band (one to three per lane-word), over
+            // the order's np planes (r = 5..8 also compare a fourth stored
+            // plane, all zero, which is not counted)
             const u32 live = 1u + (alive[1] != 0u) + (alive[2] != 0u);
             ++q.words;
-            q.tests += live * (u32)NPP * run_stages<NPP, T>(S, ia + ubias, dd, t, alive);
+            q.tests += live * np * run_stages<NPP, T>(S, ia + ubias, dd, t, alive);
         }
         queue_append(sb, q, ia, alive[0], d, t, lane);
         queue_append(sb, q, ia + 32u, alive[1], d, t, lane);
@@ -656,16 +658,16 @@ __device__ __forceinline__ void filter_item(const ProfCtx &c, const Item &it, co
             // the anchor stage counts CZ_TS* (the default tuning's) run with t fixed at compile time
             bool done;
             if constexpr (NPP == 1) {
-                done = it.t == CZ_TS1 ? filter_row_tile<1, CZ_TS1>(v, it, d, base, sb, q, lane)
-                                      : filter_row_tile<1, 0>(v, it, d, base, sb, q, lane);
+                done = it.t == CZ_TS1 ? filter_row_tile<1, CZ_TS1>(v, it, d, base, sb, q, lane, c.np)
+                                      : filter_row_tile<1, 0>(v, it, d, base, sb, q, lane, c.np);
             } else if constexpr (NPP == 2) {
-                done = it.t == CZ_TS2A ? filter_row_tile<2, CZ_TS2A>(v, it, d, base, sb, q, lane)
-                     : it.t == CZ_TS2B ? filter_row_tile<2, CZ_TS2B>(v, it, d, base, sb, q, lane)
-                                       : filter_row_tile<2, 0>(v, it, d, base, sb, q, lane);
+                done = it.t == CZ_TS2A ? filter_row_tile<2, CZ_TS2A>(v, it, d, base, sb, q, lane, c.np)
+                     : it.t == CZ_TS2B ? filter_row_tile<2, CZ_TS2B>(v, it, d, base, sb, q, lane, c.np)
+                                       : filter_row_tile<2, 0>(v, it, d, base, sb, q, lane, c.np);
             } else {
-                done = it.t == CZ_TS4A ? filter_row_tile<4, CZ_TS4A>(v, it, d, base, sb, q, lane)
-                     : it.t == CZ_TS4B ? filter_row_tile<4, CZ_TS4B>(v, it, d, base, sb, q, lane)
-                                       : filter_row_tile<4, 0>(v, it, d, base, sb, q, lane);
+                done = it.t == CZ_TS4A ? filter_row_tile<4, CZ_TS4A>(v, it, d, base, sb, q, lane, c.np)
+                     : it.t == CZ_TS4B ? filter_row_tile<4, CZ_TS4B>(v, it, d, base, sb, q, lane, c.np)
+                                       : filter_row_tile<4, 0>(v, it, d, base, sb, q, lane, c.np);
             }
             while (q.nscr >= 32u) screen_batch<NPP>(c, sb, cb, q, 32u, screen, st, lane);
             if (done) break;

@@ -26,10 +26,13 @@ every prime, through the certified rational-anchor filter.  Metric: profiles/s.
             (`moment_worker`), built from its sources into oracle/_ref, on a
             seeded sample of whole primes of the same workload (every
             admissible order of each, >= 256 profiles), on all host cores;
-  c4, c5    (one GPU, unless --quick) the batched uneven census of 64 blocks
-            of 4096 primes against one block per call, and the serving stream
-            of 10,000 requests against plain per-request calls, each with its
-            own clock record.
+  c4, c2, c5
+            (one GPU, unless --quick) the batched uneven census of 64 blocks
+            of 4096 primes against one block per call; the C2 block (4096
+            primes from 16,777,259) through the dense scan, with its Montgomery
+            roofline, and in auto mode, records compared; and the serving
+            stream of 10,000 requests against plain per-request calls -- each
+            with its own clock record.
 
 Multi-GPU (torchrun): every rank censuses its own 4096-prime block (rank k
 takes the 4096 primes below rank k-1's block): independent blocks, no
@@ -102,6 +105,53 @@ def c4_measure(eng, steps: int, warmup: int) -> dict:
         "e2e": round(nprof / (sum(e2e) / len(e2e)), 1),
         "plain_one_block_per_call": {"value": round(nprof / plain_dev, 1), "e2e": round(nprof / plain_e2e, 1)},
         "batched_over_plain": round(plain_dev / mean_dev, 3), "bit_identical": same}
+
+
+def c2_measure(eng, steps: int, warmup: int) -> dict:
+    """C2: the 4096 primes from 16,777,259, certified, with A4 -- through the
+    dense scan (every x of each half interval; the independent check) and in
+    auto mode (these primes route to the anchor filter); the two record sets
+    are compared bit for bit.  The dense scan's algorithmic work is one power
+    x^e per x in [1, (p-1)/2], e = (p-1)/m, of bitlen(e) + popcount(e) - 2
+    Montgomery products, rated against the measured Montgomery peak."""
+    from math import gcd
+    from rabung_atlas32_b200 import sieve
+    ps = sieve.primes_from(16777259, BLOCK)
+    nprof = eng.count_profiles(ps)
+    products = 0
+    for p in ps:
+        m = 1
+        for r in range(2, 10):
+            if (p - 1) % r == 0:
+                m = m * r // gcd(m, r)
+        e = (p - 1) // m
+        products += ((p - 1) // 2) * (e.bit_length() + bin(e).count("1") - 2)
+    out = {"metric": "profiles/s, C2 block (4096 primes from 16,777,259, certified, A4)", "primes": len(ps),
+           "profiles": nprof}
+    recs = {}
+    for mode in ("dense", "auto"):
+        for _ in range(max(1, warmup)):
+            eng.raw(ps, mode=mode, a4=True)
+        dev, kern = [], []
+        for _ in range(steps):
+            o, a4, st = eng.raw(ps, mode=mode, a4=True)
+            dev.append(st["ms_device"])
+            kern.append(st["ms_dense"] if mode == "dense" else st["ms_sparse"])
+        recs[mode] = [(x.p, x.r, x.M, x.L, x.witness, x.K) for x in o[:nprof]] + [tuple(a4)]
+        ms = sum(dev) / len(dev)
+        leg = {"value": round(nprof / (ms / 1000.0), 1), "unit": "profiles/s", "ms_device": round(ms, 3),
+               "kernel_ms": round(sum(kern) / len(kern), 3)}
+        if mode == "dense":
+            peak = eng.microbench(1)
+            rate = products / (leg["kernel_ms"] / 1000.0)
+            leg["roofline"] = {"bound": "int_mul", "kernel": "dense_scan_kernel", "achieved": round(rate / 1e9, 2),
+                               "peak": round(peak / 1e9, 2), "unit": "G Montgomery products/s",
+                               "frac": round(rate / peak, 4),
+                               "algorithmic": f"{products} Montgomery products per call (one power per x)",
+                               "peak_source": "measured on this GPU by cz_microbench kind 1"}
+        out[mode] = leg
+    out["dense_equals_auto"] = recs["dense"] == recs["auto"]
+    return out
 
 
 def uneven_arm(args) -> None:
@@ -477,6 +527,11 @@ def main():
             c4 = c4_measure(eng, steps=2, warmup=1)
             c4["clocks"] = ck.stop()
             out["c4"] = c4
+            ck = ClockSampler(local)
+            ck.start()
+            c2 = c2_measure(eng, steps=2, warmup=1)
+            c2["clocks"] = ck.stop()
+            out["c2"] = c2
             from rabung_atlas32_b200 import serving
             ck = ClockSampler(local)
             ck.start()

@@ -168,6 +168,19 @@ def test_refusal_on_composite(eng):
     assert time.perf_counter() - t0 < 5.0
 
 
+def test_filter_counters_cover_the_plane_pool(eng):
+    """The in-run traffic figure (cz_stats.staged_bytes, the bench's
+    roofline.traffic) counts every tile the filter copies into shared memory:
+    tiles cover every word of both views of every profile, so one sparse call
+    stages at least its whole plane pool; the filter's work counters are
+    positive and the tests are at least one stage per counted lane-word."""
+    ps = sieve.primes_ending(4294967291, 32)
+    _, _, st = eng.raw(ps, mode="sparse", a4=False)
+    pool = eng.plane_bytes(ps, mode="sparse")
+    assert pool > 0 and st["staged_bytes"] >= pool
+    assert st["words"] > 0 and st["tests"] >= st["words"] and st["completions"] > 0
+
+
 def test_replay_bit_identical(eng):
     ps = sieve.primes_ending(4294967291, 64)
     a = eng.profiles(ps, mode="sparse", a4=False)

@@ -174,6 +174,16 @@ def max_over_ranks(values: list, dist=None, device=None) -> list:
     return [float(x) for x in t]
 
 
+def sum_over_ranks(value: float, dist=None, device=None) -> float:
+    """Sum of a per-rank count (every rank gets the result)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t[0])
+
+
 def small_arm(args) -> None:
     """C1 (first 256 primes, dense) and C2 (4096 primes from 2^24, dense oracle
     and anchor filter) timings."""
@@ -445,8 +455,9 @@ def main():
     barrier()
     e2e_total = sum(e2e_ms)
     total_ms, e2e_total = max_over_ranks([total_ms, e2e_total], dist, f"cuda:{local}")
-    value = world * nprof * args.steps / (total_ms / 1000.0)
-    e2e_value = world * nprof * args.steps / (e2e_total / 1000.0)
+    all_prof = sum_over_ranks(nprof, dist, f"cuda:{local}")   # each rank's block has its own count
+    value = all_prof * args.steps / (total_ms / 1000.0)
+    e2e_value = all_prof * args.steps / (e2e_total / 1000.0)
 
     out = None
     if rank == 0:

@@ -1,6 +1,7 @@
 """Multi-process host logic of bench.py on CPU (gloo, world size 2): each rank
-takes its own disjoint block of consecutive primes (no data-path collective)
-and the step time is the maximum over ranks."""
+takes its own disjoint block of consecutive primes (no data-path collective),
+the step time is the maximum over ranks and the profiles counted are the sum
+of every rank's own block."""
 import os
 import socket
 
@@ -23,7 +24,8 @@ def _worker(rank, world, port, q):
     import bench
     ps = bench.workload(rank)
     t = bench.max_over_ranks([10.0 * (rank + 1), 1.0], dist, "cpu")
-    q.put((rank, ps[0], ps[-1], len(ps), t))
+    total = bench.sum_over_ranks(100.0 + rank, dist, "cpu")
+    q.put((rank, ps[0], ps[-1], len(ps), t, total))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -39,7 +41,8 @@ def test_two_ranks_disjoint_blocks_and_max_time():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (r0, a0, b0, n0, t0), (r1, a1, b1, n1, t1) = res
+    (r0, a0, b0, n0, t0, s0), (r1, a1, b1, n1, t1, s1) = res
     assert n0 == n1 == 4096
     assert b0 == 4294967291 and b1 < a0          # rank 1's block lies below rank 0's
     assert t0 == t1 == [20.0, 1.0]               # maximum over ranks on every rank
+    assert s0 == s1 == 201.0                     # per-rank counts summed on every rank

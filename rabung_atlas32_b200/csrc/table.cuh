@@ -203,8 +203,12 @@ table_kernel(TableArgs a) {
                     u32 cn = c + t.sig;
                     if (cn >= t.r) cn -= t.r;
                     if (n == 0u) { c = 0u; cn = 0u; }
-                    const u32 co = __shfl_sync(0xFFFFFFFFu, c, 2 * (lane & 15) + 1);
-                    const u32 cno = __shfl_sync(0xFFFFFFFFu, cn, 2 * (lane & 15) + 1);
+                    // odd numerators of the step (odd lanes): lanes 0..15 take the
+                    // colour of lane 2l + 1, lanes 16..31 its reflection, from one
+                    // shuffle of the packed pair (colours < 16), so one ballot per
+                    // plane gives both odd-view half words
+                    const u32 pk = __shfl_sync(0xFFFFFFFFu, c | (cn << 4), 2 * (lane & 15) + 1);
+                    const u32 ch = lane < 16 ? (pk & 15u) : (pk >> 4);
                     const bool odd_step = (k & 1u) != 0u;
                     // lane b collects plane b's words; one store per word kind
                     // then writes the interleaved planes of a word together
@@ -214,8 +218,8 @@ table_kernel(TableArgs a) {
                         if (b >= (int)t.npp) break;
                         const u32 wp = __ballot_sync(0xFFFFFFFFu, (c >> b) & 1u);
                         const u32 wn = __ballot_sync(0xFFFFFFFFu, (cn >> b) & 1u);
-                        const u32 hp = __ballot_sync(0xFFFFFFFFu, (co >> b) & 1u) & 0xFFFFu;
-                        const u32 hn = __ballot_sync(0xFFFFFFFFu, (cno >> b) & 1u) & 0xFFFFu;
+                        const u32 hb = __ballot_sync(0xFFFFFFFFu, (ch >> b) & 1u);
+                        const u32 hp = hb & 0xFFFFu, hn = hb >> 16;
                         if (lane == b) {
                             vneg = __brev(wn);
                             vpos = (prevw[b] >> 1) | ((wp & 1u) << 31);
